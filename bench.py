@@ -1,0 +1,386 @@
+#!/usr/bin/env python
+"""Benchmark of the fused LBM step (MLUPS and fraction of the HBM roofline).
+
+Default workload: 512x256x256 D3Q27, FP32, regularized third-order Hermite
+collision with Vreman LES, inflow/outflow in i, periodic j, no-slip bottom and
+free-slip top in k, inflow-turbulence forcing at i=10 (seeded synthetic
+fields), no solids.  One "step" is one lattice time step over the whole grid.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own independent replica (the path has no
+exchange step between replicas); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS & % of HBM roofline: FP16-offset store vs plain FP32 at stated L2 error"
+L2_NOTE = "inputs larger than L2: the two distribution buffers (7.8 GB) exceed the 126 MB L2, no flush needed"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="turb_inflow_q27_512x256x256")
+    ap.add_argument("--storage", choices=["f32", "f16"], default="f32")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-f16", action="store_true", help="skip the FP16-offset storage comparison")
+    return ap.parse_args()
+
+
+def bytes_per_lup(nl, storage):
+    return 2 * nl * (2 if storage == "f16" else 4)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(kernel_key, cells):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary,
+    scaled by cells (traffic of this streaming kernel grows with the cells)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        e = d[kernel_key]
+        return float(e["dram_bytes_per_launch"]) * cells / float(e["cells"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region (NVML, sampled from a thread)
+# ---------------------------------------------------------------------------
+REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+           0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+           0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    def __init__(self, device_index):
+        self.samples = []
+        self.reasons = 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(device_index)
+            bus = "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+            self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:   # clocks are reported as unavailable, never guessed
+            self.error = str(e)
+
+    def _reasons(self):
+        nv = self._nv
+        fn = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        return fn(self._h)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self._nv.nvmlDeviceGetClockInfo(self._h, self._nv.NVML_CLOCK_SM))
+                self.reasons |= int(self._reasons())
+            except Exception:
+                pass
+            self._stop.wait(0.02)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self._h is not None:
+            self._stop.set()
+            self._t.join()
+
+    def report(self):
+        if self._h is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "note": "NVML unavailable"}
+        names = [n for b, n in REASONS.items() if self.reasons & b and n != "gpu_idle"]
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (restatement of the reference's OpenMP CPU path)
+# ---------------------------------------------------------------------------
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def oracle_case(wl, nz_s):
+    import numpy as np
+    from lbm_b200 import workloads as W
+    from oracle import oracle as O
+    s = wl.with_(nz=nz_s)
+    cfg = O.Config(s.nx, s.ny, s.nz, s.nl, ibnd=s.ibnd, jbnd=s.jbnd, kbnd=s.kbnd, iturb_pos=10,
+                   lturb=s.lturb, nrturb=s.nrturb, ampl=s.ampl, kinevisc=s.kinevisc, smagorinsky=s.smagorinsky)
+    o = O.Oracle(cfg, np.float32)
+    rho, u, v, w = W.initial_macro(s)
+    uvel = W.inflow_profile(s)
+    fA, fB = o.zeros_f(), o.zeros_f()
+    o.init(fA, fB, rho, u, v, w, uvel)
+    tau = np.full(cfg.sshape, 3 * np.float32(s.kinevisc) + 0.5, np.float32)
+    kw = {}
+    if s.lturb:
+        uu, vv, ww = W.turbulence_fields(s.ny, s.nz, s.nrturb, s.seed)
+        kw = dict(uu=uu, vv=vv, ww=ww)
+    state = dict(fA=fA, fB=fB, rho=rho, u=u, v=v, w=w, tau=tau, uvel=uvel, kw=kw, it=0)
+
+    def run(n):
+        o.run(state["fA"], state["fB"], state["rho"], state["u"], state["v"], state["w"], state["tau"],
+              state["uvel"], n, it0=state["it"], **state["kw"])
+        state["it"] += n
+    return s, run
+
+
+def cpu_sample(wl, budget_s, steps_hint):
+    """Pick the thickest k-slab of the workload that runs steps_hint steps within budget_s."""
+    from oracle import oracle as O
+    O.set_threads(cpu_threads())
+    probe, run = oracle_case(wl, 4)
+    t0 = time.perf_counter()
+    run(1)
+    rate = probe.cells / (time.perf_counter() - t0)          # LUP/s
+    nz_s = int(budget_s * rate / (max(steps_hint, 1) * wl.nx * wl.ny))
+    return max(2, min(wl.nz, nz_s))
+
+
+def cpu_baseline(wl):
+    nz_s = cpu_sample(wl, 15.0, 3)
+    s, run = oracle_case(wl, nz_s)
+    run(1)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        run(1)
+        n += 1
+        el = time.perf_counter() - t0
+        if el > 10.0 or n >= 50:
+            break
+    mlups = s.cells * n / el / 1e6
+    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": cpu_threads(), "kind": "port",
+            "sample": "%dx%dx%d D3Q%d FP32 slab of the workload (same physics), %d steps in %.1f s, OpenMP %d threads"
+                      % (s.nx, s.ny, s.nz, s.nl, n, el, cpu_threads())}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(a, wl):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    nz_s = cpu_sample(wl, 90.0, a.warmup + a.steps)
+    s, run = oracle_case(wl, nz_s)
+    if a.warmup > 0:
+        run(a.warmup)
+    t0 = time.perf_counter()
+    run(a.steps)
+    el = time.perf_counter() - t0
+    mlups = s.cells * a.steps / el / 1e6
+    sample = ("%dx%dx%d k-slab of the %s workload, D3Q%d FP32, same physics; C++ restatement of the reference's "
+              "OpenMP CPU path (the Fortran reference has no compiler in this image)" % (s.nx, s.ny, s.nz, wl.name, s.nl))
+    line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(el / max(a.steps, 1) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(wl, "f32", a.gpus),
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cpu_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_of(wl, storage, n):
+    return {"workload": wl.name, "grid": [wl.nx, wl.ny, wl.nz], "lattice": "D3Q%d" % wl.nl, "storage": storage,
+            "collision": "regularized 3rd-order Hermite + Vreman (Cs=0.15), nu=1e-4",
+            "boundaries": "i inflow u=%.2f / outflow, j periodic, k no-slip bottom + free-slip top" % wl.uin,
+            "forcing": "inflow turbulence at i=10, ampl=%g, nrturb=%d" % (wl.ampl, wl.nrturb) if wl.lturb else "none",
+            "l2": L2_NOTE, "parallelism": "replicas x%d" % n if n > 1 else "single GPU"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def make_solver(wl, storage, seed):
+    import torch
+    from lbm_b200 import Params, Solver, workloads as W
+    w2 = wl.with_(seed=seed)
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(w2))
+    uvel = torch.from_numpy(W.inflow_profile(w2)).cuda()
+    tb = None
+    if w2.lturb:
+        uu, vv, ww = (torch.from_numpy(x).cuda() for x in W.turbulence_fields(w2.ny, w2.nz, w2.nrturb, w2.seed))
+        tb = (uu, vv, ww, w2.nrturb, w2.ampl)
+    p = Params(nx=w2.nx, ny=w2.ny, nz=w2.nz, nl=w2.nl, ibnd=w2.ibnd, jbnd=w2.jbnd, kbnd=w2.kbnd,
+               kinevisc=w2.kinevisc, smagorinsky=w2.smagorinsky, iturb_pos=10, storage=storage)
+    s = Solver(p, rho, u, v, w, uvel, blanking=None, turbulence=tb)
+    del rho, u, v, w
+    torch.cuda.synchronize()
+    return s
+
+
+def timed_steps(s, steps, dist, profile=True):
+    """Time exactly `steps` fused steps with CUDA events on the library's stream; max over ranks."""
+    import torch
+    L = s.lbm
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    L.profile(profile)
+    n0 = L.launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(L.stream)
+    s.step(steps)
+    e1.record(L.stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    launched = L.launches - n0
+    kms, kn = L.profile_read() if profile else (0.0, 0)
+    L.profile(False)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    return ms, launched, kms, kn
+
+
+def e2e_steps(s, steps, wl, dist):
+    """End to end through the public host-buffer entry point: every step copies the
+    inflow profile from pinned host memory and reads the status word back."""
+    import torch
+    from lbm_b200 import workloads as W
+    uvel_host = torch.from_numpy(W.inflow_profile(wl)).pin_memory()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bad = 0
+    for _ in range(steps):
+        bad |= s.lbm.step_host(1, uvel_host)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        el = float(t.item())
+    return el, bad, wl.nz * 4, 4
+
+
+def main():
+    a = parse()
+    from lbm_b200 import workloads as W
+    wl = W.WORKLOADS[a.workload]
+    if a.impl == "reference":
+        return run_reference(a, wl)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    s = make_solver(wl, a.storage, seed=wl.seed + rank)
+    s.step(a.warmup)
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        ms, launched, kms, kn = timed_steps(s, a.steps, dist)
+    st = s.lbm.status()
+    cells = wl.cells
+    value = world * cells * a.steps / (ms * 1e-3) / 1e6
+    hbm, hbm_kind = peaks()
+    bl = bytes_per_lup(wl.nl, a.storage)
+    k_ms = kms / max(kn, 1)
+    achieved = cells * bl / (k_ms * 1e-3) / 1e9 if kn else None
+    key = "k_step<%d,%s,true>" % (wl.nl, "float" if a.storage == "f32" else "__half")
+    traffic = ncu_traffic(key, cells)
+    line = {"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if a.storage == "f32" else "f16-storage/f32-compute",
+            "data": "synthetic (seeded initial field, seeded smooth inflow-turbulence fields)",
+            "config": config_of(wl, a.storage, world),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1) if achieved else None, "peak": hbm,
+                         "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
+                         "traffic": traffic, "peak_kind": hbm_kind,
+                         "kernel": key, "kernel_ms": round(k_ms, 4), "kernel_launches": kn,
+                         "algorithmic_bytes_per_launch": cells * bl,
+                         "note": "frac of %s HBM copy bandwidth; traffic = ncu dram bytes per launch" % hbm_kind},
+            "gpu_launches": launched, "clocks": clk.report(), "status_flags": st}
+
+    if not a.no_e2e:
+        el, bad, h2d, d2h = e2e_steps(s, a.steps, wl, dist)
+        line["e2e"] = {"value": round(world * cells * a.steps / el / 1e6, 1), "unit": "MLUPS",
+                       "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                       "api": "lbm_step_host (uvel host->device, status word device->host, per step)"}
+    s.close()
+    del s
+    torch.cuda.empty_cache()
+
+    if not a.no_f16 and a.storage == "f32" and world == 1:
+        s16 = make_solver(wl, "f16", seed=wl.seed + rank)
+        s16.step(a.warmup)
+        ms16, _, kms16, kn16 = timed_steps(s16, a.steps, dist)
+        s16.close()
+        v16 = world * cells * a.steps / (ms16 * 1e-3) / 1e6
+        ach16 = cells * bytes_per_lup(wl.nl, "f16") / (kms16 / max(kn16, 1) * 1e-3) / 1e9 if kn16 else None
+        line["f16_storage"] = {"value": round(v16, 1), "unit": "MLUPS", "speedup_vs_f32": round(v16 / value, 3),
+                               "roofline_frac": round(ach16 / hbm, 4) if ach16 else None,
+                               "kernel_ms": round(kms16 / max(kn16, 1), 4)}
+        torch.cuda.empty_cache()
+
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

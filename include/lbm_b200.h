@@ -1,0 +1,173 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 (sm_100a) LBM per-timestep library.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Per-call entry points with the reference's subroutine interfaces
+ *     (geirev/LBM, the src/ Fortran sources).  Arrays are DEVICE pointers in the reference
+ *     layout: f(nl,0:nx+1,0:ny+1,0:nz+1) column-major (l fastest), scalars
+ *     (0:nx+1,0:ny+1,0:nz+1), uvel(nz), ablvisc(nz), uu/vv/ww(ny,nz,0:nrturb),
+ *     turbulence_df(nl,ny,nz), lblanking logical(4).  Fortran passes arrays by
+ *     reference, so each Fortran dummy array becomes one C pointer.  The
+ *     caller owns every buffer.  Dimensions and options come from the context
+ *     (the reference takes them from module variables).
+ *
+ *  2. A fused state API: the context owns a structure-of-arrays copy of the
+ *     two distribution buffers and advances whole time steps with one fused
+ *     kernel per step (streaming, moments, equilibrium, regularized
+ *     collision, Vreman, turbulence forcing, solids) followed by the
+ *     boundary-condition kernels, in the reference's step order
+ *     (main.F90:288-329).
+ *
+ * Conventions: every entry point returns LBM_OK (0) or a negative LBM_ERR_*
+ * code and never traps; lbm_last_error() gives the message.  All work is
+ * stream-ordered on the context's stream (the legacy default stream unless
+ * lbm_set_stream names another); entry points that return results to host
+ * memory synchronise that stream.  Floating-point data is FP32, the
+ * reference's default precision.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_B200_ABI_VERSION 1
+
+enum {
+    LBM_OK = 0,
+    LBM_ERR_ARG = -1,          /* bad argument, dimension or null pointer  */
+    LBM_ERR_UNSUPPORTED = -2,  /* option the library does not implement   */
+    LBM_ERR_CUDA = -3,         /* CUDA runtime error                       */
+    LBM_ERR_STATE = -4,        /* call out of order (e.g. step before import) */
+    LBM_ERR_NUMERIC = -5,      /* NaN/Inf or non-positive density detected */
+    LBM_ERR_OOM = -6           /* device allocation failed                 */
+};
+
+/* storage of the fused state */
+enum {
+    LBM_STORE_F32 = 0,     /* f - w_l stored in FP32                          */
+    LBM_STORE_F16 = 1      /* (f - w_l) * 2^8 stored in FP16, computed in FP32 */
+};
+
+/* status bits returned by lbm_status() */
+enum {
+    LBM_STATUS_BAD_DENSITY = 1   /* some cell had rho <= 0, NaN or Inf (m_rhotest.F90) */
+};
+
+/* Run-time options.  Field meanings follow m_readinfile.F90:3-58 and
+ * mod_dimensions.F90; values are in lattice units. */
+typedef struct lbm_params {
+    int32_t nx, ny, nz;     /* interior grid; ghosts add one cell per side      */
+    int32_t nl;             /* 19 (D3Q19) or 27 (D3Q27)                          */
+    int32_t ibgk;           /* 2 or 3: order of the Hermite equilibrium          */
+    int32_t ihrr;           /* 1: regularized non-equilibrium R(fneq)            */
+    int32_t ivreman;        /* 1: Vreman eddy viscosity                          */
+    int32_t ibnd, jbnd, kbnd; /* 0 periodic, 1 inflow/outflow (i only), 11,12,21,22 closed */
+    int32_t iturb_pos;      /* i index of the turbulence forcing slice (10)      */
+    int32_t storage;        /* LBM_STORE_F32 or LBM_STORE_F16 (fused state only) */
+    float kinevisc;         /* kinematic viscosity                               */
+    float smagorinsky;      /* model constant; Vreman uses 2.5*smagorinsky^2     */
+    float rho0;             /* reference density (1.0)                           */
+    float udir;             /* inflow direction, degrees                         */
+} lbm_params;
+
+typedef struct lbm_ctx lbm_ctx;
+
+/* ---- context --------------------------------------------------------------- */
+int lbm_create(lbm_ctx** ctx, const lbm_params* p);
+int lbm_destroy(lbm_ctx* ctx);
+const char* lbm_last_error(const lbm_ctx* ctx);
+int lbm_abi_version(void);
+/* stream is a cudaStream_t for all later work of the context; NULL (the default)
+ * is the legacy default stream, where the reference launches its kernels */
+int lbm_set_stream(lbm_ctx* ctx, void* stream);
+int lbm_synchronize(lbm_ctx* ctx);
+
+/* ---- per-call entry points (reference interfaces) -------------------------- */
+
+/* fequil3(feq,rho,u,v,w)           m_fequil3.F90:4; kernel m_fequil3_kernel.F90:7 */
+int lbm_fequil3(lbm_ctx* ctx, float* feq, const float* rho, const float* u, const float* v, const float* w);
+
+/* postcoll(f,tau,rho,u,v,w)        m_postcoll.F90:4; kernel m_postcoll_kernel.F90:7.
+ * ablvisc(nz) replaces the module array m_mechanical_ablvisc::ablvisc (may be NULL = 0). */
+int lbm_postcoll(lbm_ctx* ctx, float* f, float* tau, const float* rho, const float* u, const float* v,
+                 const float* w, const float* ablvisc);
+
+/* drift(f,feq): f = streamed feq     m_drift.F90:3; kernel m_drift_kernel.F90:7 */
+int lbm_drift(lbm_ctx* ctx, float* f, const float* feq);
+
+/* macrovars(rho,u,v,w,f)           m_macrovars.F90:4; kernel m_macrovars_kernel.F90:6 */
+int lbm_macrovars(lbm_ctx* ctx, float* rho, float* u, float* v, float* w, const float* f);
+
+/* regularization(f,feq,u,v,w): f = R(f - feq)   m_regularization.F90:4 */
+int lbm_regularization(lbm_ctx* ctx, float* f, const float* feq, const float* u, const float* v, const float* w);
+
+/* vreman(f,tau): tau from non-equilibrium f     m_vreman.F90:187 */
+int lbm_vreman(lbm_ctx* ctx, const float* f, float* tau);
+
+/* compute_fneq(f,feq): f = f - feq              m_compute_fneq.F90:4 */
+int lbm_compute_fneq(lbm_ctx* ctx, float* f, const float* feq);
+
+/* compute_f(f,feq): f = feq + f                 m_compute_f.F90:84 */
+int lbm_compute_f(lbm_ctx* ctx, float* f, const float* feq);
+
+/* boundarycond(f1,f2,uvel,...)     m_boundarycond.F90:14 (tracer/pottemp are off this path) */
+int lbm_boundarycond(lbm_ctx* ctx, float* f1, float* f2, const float* uvel);
+
+/* solids(f,blanking)               m_solids.F90:3; blanking is logical(4) over the ghost-inclusive grid */
+int lbm_solids(lbm_ctx* ctx, float* f, const int32_t* blanking);
+
+/* inflow_turbulence_forcing(rho,u,v,w,ampl,it,nrturb)  m_inflow_turbulence_forcing.F90:5.
+ * The reference keeps turbulence_df and uu,vv,ww in module m_inflow_turbulence_init;
+ * here they are explicit arguments: df(nl,ny,nz) out, uu/vv/ww(ny,nz,0:nrturb) in. */
+int lbm_inflow_turbulence_forcing(lbm_ctx* ctx, float* df, const float* rho, const float* u, const float* v,
+                                  const float* w, const float* uu, const float* vv, const float* ww,
+                                  float ampl, int32_t it, int32_t nrturb);
+
+/* inflow_turbulence_apply(f,turbulence_df)      m_inflow_turbulence_apply.F90:4 */
+int lbm_inflow_turbulence_apply(lbm_ctx* ctx, float* f, const float* df);
+
+/* fillghosts(f)                    m_fillghosts.F90:4 */
+int lbm_fillghosts(lbm_ctx* ctx, float* f);
+
+/* ---- fused state API ---------------------------------------------------------
+ * The state mirrors main.F90 between time steps: f1 (pre-collision, after
+ * drift), f2 (the previous post-collision buffer with its ghost cells), and
+ * rho,u,v,w (the moments postcoll will use).  `it` is the number of the last
+ * completed step (nt0 after initialisation). */
+int lbm_state_import(lbm_ctx* ctx, const float* f1, const float* f2, const float* rho, const float* u,
+                     const float* v, const float* w, int32_t it);
+int lbm_state_export(lbm_ctx* ctx, float* f1, float* f2);
+/* rho,u,v,w of the current state over the ghost-inclusive grid (macrovars of f1) */
+int lbm_get_macro(lbm_ctx* ctx, float* rho, float* u, float* v, float* w);
+/* solid mask for solids() inside the step; NULL removes it */
+int lbm_set_solids(lbm_ctx* ctx, const int32_t* blanking);
+/* inflow turbulence inside the step; uu == NULL disables it */
+int lbm_set_turbulence(lbm_ctx* ctx, const float* uu, const float* vv, const float* ww, int32_t nrturb, float ampl);
+/* inflow profile uvel(nz) (device pointer) used by boundarycond from the next step on */
+int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
+/* advance nsteps time steps */
+int lbm_step(lbm_ctx* ctx, int32_t nsteps);
+/* host-buffer step: copies uvel(nz) from host memory before each step (NULL keeps the
+ * current profile), runs nsteps steps, and writes the status word to *status_host */
+int lbm_step_host(lbm_ctx* ctx, int32_t nsteps, const float* uvel_host, int32_t* status_host);
+int lbm_get_step(lbm_ctx* ctx, int32_t* it);
+/* accumulated LBM_STATUS_* bits since the last call; synchronises and clears them */
+int lbm_status(lbm_ctx* ctx, int32_t* flags);
+
+/* ---- instrumentation (no counterpart in the reference, whose timers are m_wtime.F90) ---- */
+/* number of kernel launches this context has issued */
+int lbm_launch_count(lbm_ctx* ctx, int64_t* n);
+/* enable (1) or disable (0) CUDA-event timing of every fused step-kernel launch; resets the totals */
+int lbm_profile(lbm_ctx* ctx, int32_t enable);
+/* synchronise and return the summed device time and number of timed step-kernel launches */
+int lbm_profile_read(lbm_ctx* ctx, double* step_kernel_ms, int64_t* step_kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,270 @@
+"""Python mirror of the reference's subroutine interfaces over the C ABI.
+
+Each method of :class:`Lbm` is named after the Fortran subroutine it replaces
+and takes the same arrays in the same order (geirev/LBM src/*.F90), as CUDA
+torch tensors in the reference layout viewed in C order:
+
+* ``f(nl,0:nx+1,0:ny+1,0:nz+1)`` -> ``float32[nz+2, ny+2, nx+2, nl]``
+* ``rho(0:nx+1,0:ny+1,0:nz+1)``  -> ``float32[nz+2, ny+2, nx+2]``
+* ``uvel(nz)``, ``ablvisc(nz)``  -> ``float32[nz]``
+* ``uu(ny,nz,0:nrturb)``          -> ``float32[nrturb+1, nz, ny]``
+* ``turbulence_df(nl,ny,nz)``     -> ``float32[nz, ny, nl]``
+* ``lblanking`` logical(4)        -> ``int32[nz+2, ny+2, nx+2]``
+
+torch is used for device memory and streams only; all arithmetic runs in the
+library's sm_100a kernels.  Errors raise :class:`LbmError`.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import torch
+
+from . import _lib
+from ._lib import LbmError, LbmParams
+
+
+@dataclasses.dataclass
+class Params:
+    """Run-time options (m_readinfile.F90:3-58, mod_dimensions.F90), lattice units."""
+    nx: int
+    ny: int
+    nz: int
+    nl: int = 27
+    ibgk: int = 3
+    ihrr: int = 1
+    ivreman: int = 1
+    ibnd: int = 1
+    jbnd: int = 0
+    kbnd: int = 12
+    iturb_pos: int = 10
+    storage: str = "f32"          # fused state storage: "f32" or "f16" (offsets scaled by 2^8)
+    kinevisc: float = 1.0e-4
+    smagorinsky: float = 0.15
+    rho0: float = 1.0
+    udir: float = 0.0
+
+    def c(self) -> LbmParams:
+        st = {"f32": _lib.LBM_STORE_F32, "f16": _lib.LBM_STORE_F16}[self.storage]
+        return LbmParams(self.nx, self.ny, self.nz, self.nl, self.ibgk, self.ihrr, self.ivreman, self.ibnd,
+                         self.jbnd, self.kbnd, self.iturb_pos, st, self.kinevisc, self.smagorinsky, self.rho0,
+                         self.udir)
+
+    @property
+    def fshape(self):
+        return (self.nz + 2, self.ny + 2, self.nx + 2, self.nl)
+
+    @property
+    def sshape(self):
+        return (self.nz + 2, self.ny + 2, self.nx + 2)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Lbm:
+    """One context of the C library (``lbm_create``) bound to the current CUDA device."""
+
+    def __init__(self, params: Params, stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("lbm_b200 needs a CUDA device; there is no CPU fallback")
+        self.p = params
+        self.L = _lib.load()
+        self._cp = params.c()
+        h = ctypes.c_void_p()
+        rc = self.L.lbm_create(ctypes.byref(h), ctypes.byref(self._cp))
+        if rc != 0:
+            raise LbmError(rc, "lbm_create failed for %s" % (params,))
+        self.h = h
+        self.stream = stream if stream is not None else torch.cuda.current_stream()
+        self._call("lbm_set_stream", ctypes.c_void_p(self.stream.cuda_stream))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- helpers ---------------------------------------------------------------
+    def _call(self, name, *args):
+        rc = getattr(self.L, name)(self.h, *args)
+        if rc != 0:
+            raise LbmError(rc, self.L.lbm_last_error(self.h).decode())
+        return rc
+
+    def _chk(self, t, shape, dtype=torch.float32, name="array"):
+        if t is None:
+            return
+        if not t.is_cuda:
+            raise LbmError(_lib.LBM_ERR_ARG, "%s must be a CUDA tensor" % name)
+        if t.dtype != dtype or tuple(t.shape) != tuple(shape) or not t.is_contiguous():
+            raise LbmError(_lib.LBM_ERR_ARG, "%s must be contiguous %s%s, got %s%s" % (
+                name, dtype, tuple(shape), t.dtype, tuple(t.shape)))
+
+    def _f(self, *ts):
+        for t in ts:
+            self._chk(t, self.p.fshape, name="f")
+
+    def _s(self, *ts):
+        for t in ts:
+            self._chk(t, self.p.sshape, name="scalar field")
+
+    # ---- tensors -----------------------------------------------------------------
+    def empty_f(self):
+        return torch.zeros(self.p.fshape, dtype=torch.float32, device="cuda")
+
+    def empty_s(self):
+        return torch.zeros(self.p.sshape, dtype=torch.float32, device="cuda")
+
+    # ---- reference subroutines -------------------------------------------------------
+    def fequil3(self, feq, rho, u, v, w):
+        self._f(feq)
+        self._s(rho, u, v, w)
+        self._call("lbm_fequil3", _ptr(feq), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+
+    def postcoll(self, f, tau, rho, u, v, w, ablvisc=None):
+        self._f(f)
+        self._s(tau, rho, u, v, w)
+        self._chk(ablvisc, (self.p.nz,), name="ablvisc")
+        self._call("lbm_postcoll", _ptr(f), _ptr(tau), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(ablvisc))
+
+    def drift(self, f, feq):
+        self._f(f, feq)
+        self._call("lbm_drift", _ptr(f), _ptr(feq))
+
+    def macrovars(self, rho, u, v, w, f):
+        self._s(rho, u, v, w)
+        self._f(f)
+        self._call("lbm_macrovars", _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(f))
+
+    def regularization(self, f, feq, u, v, w):
+        self._f(f, feq)
+        self._s(u, v, w)
+        self._call("lbm_regularization", _ptr(f), _ptr(feq), _ptr(u), _ptr(v), _ptr(w))
+
+    def vreman(self, f, tau):
+        self._f(f)
+        self._s(tau)
+        self._call("lbm_vreman", _ptr(f), _ptr(tau))
+
+    def compute_fneq(self, f, feq):
+        self._f(f, feq)
+        self._call("lbm_compute_fneq", _ptr(f), _ptr(feq))
+
+    def compute_f(self, f, feq):
+        self._f(f, feq)
+        self._call("lbm_compute_f", _ptr(f), _ptr(feq))
+
+    def boundarycond(self, f1, f2, uvel):
+        self._f(f1, f2)
+        self._chk(uvel, (self.p.nz,), name="uvel")
+        self._call("lbm_boundarycond", _ptr(f1), _ptr(f2), _ptr(uvel))
+
+    def solids(self, f, blanking):
+        self._f(f)
+        self._chk(blanking, self.p.sshape, torch.int32, name="blanking")
+        self._call("lbm_solids", _ptr(f), _ptr(blanking))
+
+    def inflow_turbulence_forcing(self, df, rho, u, v, w, uu, vv, ww, ampl, it, nrturb):
+        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
+        self._s(rho, u, v, w)
+        for t in (uu, vv, ww):
+            self._chk(t, (nrturb + 1, self.p.nz, self.p.ny), name="uu/vv/ww")
+        self._call("lbm_inflow_turbulence_forcing", _ptr(df), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(uu),
+                   _ptr(vv), _ptr(ww), ctypes.c_float(ampl), ctypes.c_int32(it), ctypes.c_int32(nrturb))
+
+    def inflow_turbulence_apply(self, f, df):
+        self._f(f)
+        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
+        self._call("lbm_inflow_turbulence_apply", _ptr(f), _ptr(df))
+
+    def fillghosts(self, f):
+        self._f(f)
+        self._call("lbm_fillghosts", _ptr(f))
+
+    # ---- fused state ------------------------------------------------------------------
+    def state_import(self, f1, f2, rho, u, v, w, it=0):
+        self._f(f1, f2)
+        self._s(rho, u, v, w)
+        self._call("lbm_state_import", _ptr(f1), _ptr(f2), _ptr(rho), _ptr(u), _ptr(v), _ptr(w),
+                   ctypes.c_int32(it))
+
+    def state_export(self, f1, f2):
+        self._f(f1, f2)
+        self._call("lbm_state_export", _ptr(f1), _ptr(f2))
+
+    def get_macro(self, rho, u, v, w):
+        self._s(rho, u, v, w)
+        self._call("lbm_get_macro", _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+
+    def set_solids(self, blanking):
+        self._chk(blanking, self.p.sshape, torch.int32, name="blanking")
+        self._call("lbm_set_solids", _ptr(blanking))
+
+    def set_turbulence(self, uu, vv, ww, nrturb, ampl):
+        if uu is None:
+            self._call("lbm_set_turbulence", None, None, None, ctypes.c_int32(0), ctypes.c_float(0.0))
+            return
+        for t in (uu, vv, ww):
+            self._chk(t, (nrturb + 1, self.p.nz, self.p.ny), name="uu/vv/ww")
+        self._call("lbm_set_turbulence", _ptr(uu), _ptr(vv), _ptr(ww), ctypes.c_int32(nrturb),
+                   ctypes.c_float(ampl))
+
+    def set_inflow(self, uvel):
+        self._chk(uvel, (self.p.nz,), name="uvel")
+        self._call("lbm_set_inflow", _ptr(uvel))
+
+    def step(self, nsteps=1):
+        self._call("lbm_step", ctypes.c_int32(nsteps))
+
+    def step_host(self, nsteps, uvel_host=None):
+        """Steps with host buffers: uvel_host is a CPU float32 tensor (pinned for async copies)."""
+        st = ctypes.c_int32(0)
+        if uvel_host is not None:
+            if uvel_host.is_cuda or uvel_host.dtype != torch.float32 or tuple(uvel_host.shape) != (self.p.nz,):
+                raise LbmError(_lib.LBM_ERR_ARG, "uvel_host must be a CPU float32 tensor of shape (nz,)")
+        self._call("lbm_step_host", ctypes.c_int32(nsteps), _ptr(uvel_host), ctypes.byref(st))
+        return st.value
+
+    @property
+    def it(self):
+        v = ctypes.c_int32()
+        self._call("lbm_get_step", ctypes.byref(v))
+        return v.value
+
+    def status(self):
+        v = ctypes.c_int32()
+        self._call("lbm_status", ctypes.byref(v))
+        return v.value
+
+    def synchronize(self):
+        self._call("lbm_synchronize")
+
+    # ---- instrumentation -------------------------------------------------------------
+    @property
+    def launches(self):
+        v = ctypes.c_int64()
+        self._call("lbm_launch_count", ctypes.byref(v))
+        return v.value
+
+    def profile(self, enable=True):
+        self._call("lbm_profile", ctypes.c_int32(1 if enable else 0))
+
+    def profile_read(self):
+        """(summed device ms, launches) of the fused step kernel since profile(True)."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        self._call("lbm_profile_read", ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value

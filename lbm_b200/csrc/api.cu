@@ -1,0 +1,824 @@
+// api.cu -- C ABI of the B200 LBM library (declarations in include/lbm_b200.h).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "boundary.cuh"
+#include "ref_kernels.cuh"
+#include "state_kernels.cuh"
+
+using namespace lbm;
+
+enum { ST_NONE = 0, ST_PRE = 1, ST_POST = 2 };
+
+struct lbm_ctx {
+    lbm_params p;
+    int dev = 0;
+    cudaStream_t stream = nullptr;   // legacy default stream unless lbm_set_stream gives another
+    std::string err;
+    RefGrid rg;
+    SoaGrid sg;
+    CollideParams cp;
+    FacePairs face[3][2];
+    bool face_on[3] = {false, false, false};
+    EdgeSet edges[3];
+    bool edges_on[3] = {false, false, false};
+    CornerSet corners;
+    bool corners_on = false;
+    float cosd = 1.f, sind = 0.f;
+    // fused state
+    void* buf[2] = {nullptr, nullptr};
+    size_t elem = 4;
+    int cur = 0;
+    int state = ST_NONE;
+    float* d_macro = nullptr;     // rho,u,v,w (4 x ghost-inclusive grid) of an imported state
+    uint8_t* d_solid = nullptr;   // interior solid mask
+    float* d_turb = nullptr;      // uu,vv,ww copies
+    int nrturb = 0;
+    float ampl = 0.f;
+    float* d_uvel = nullptr;      // uvel(nz)
+    float* d_abl = nullptr;       // ablvisc(nz), zero unless set
+    int* d_it = nullptr;          // number of the step being computed
+    int* d_status = nullptr;
+    int it = 0;
+    // instrumentation: kernel launches issued, optional event timing of the step kernel
+    long long launches = 0;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev;   // pairs (start, stop)
+    size_t ev_used = 0;
+    double prof_ms = 0.0;
+    long long prof_launches = 0;
+};
+
+namespace {
+
+int fail(lbm_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int cuda_check(lbm_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return LBM_OK;
+    return fail(c, e == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define LBM_TRY(...)                    \
+    do {                                \
+        int _rc = (__VA_ARGS__);        \
+        if (_rc != LBM_OK) return _rc;  \
+    } while (0)
+#define LBM_LAUNCHED(c, what) LBM_TRY(cuda_check((c), cudaPeekAtLastError(), (what)))
+
+// accumulate the elapsed time of recorded event pairs, then reuse them
+int prof_drain(lbm_ctx* c) {
+    if (c->ev_used == 0) return LBM_OK;
+    int rc = cuda_check(c, cudaEventSynchronize(c->ev[2 * c->ev_used - 1]), "profile");
+    if (rc != LBM_OK) return rc;
+    for (size_t q = 0; q < c->ev_used; ++q) {
+        float ms = 0.f;
+        rc = cuda_check(c, cudaEventElapsedTime(&ms, c->ev[2 * q], c->ev[2 * q + 1]), "profile");
+        if (rc != LBM_OK) return rc;
+        c->prof_ms += ms;
+    }
+    c->ev_used = 0;
+    return LBM_OK;
+}
+int prof_begin(lbm_ctx* c) {
+    if (!c->profiling) return LBM_OK;
+    if (c->ev_used * 2 >= c->ev.size()) LBM_TRY(prof_drain(c));
+    return cuda_check(c, cudaEventRecord(c->ev[2 * c->ev_used], c->stream), "profile");
+}
+int prof_end(lbm_ctx* c) {
+    if (!c->profiling) return LBM_OK;
+    LBM_TRY(cuda_check(c, cudaEventRecord(c->ev[2 * c->ev_used + 1], c->stream), "profile"));
+    c->ev_used++;
+    c->prof_launches++;
+    return LBM_OK;
+}
+#define NEED(c, ptr) \
+    if ((ptr) == nullptr) return fail((c), LBM_ERR_ARG, "%s: null pointer argument '%s'", __func__, #ptr)
+
+int lat_find(int nl, int x, int y, int z) {
+    for (int m = 0; m < nl; ++m)
+        if (lat_cx(m) == x && lat_cy(m) == y && lat_cz(m) == z) return m;
+    return -1;
+}
+
+void closed_opts(int code, int& o1, int& oN) {
+    switch (code) {
+        case 11: o1 = -1; oN = -1; break;
+        case 12: o1 = -1; oN = +1; break;
+        case 21: o1 = +1; oN = -1; break;
+        case 22: o1 = +1; oN = +1; break;
+        default: o1 = 0; oN = 0;
+    }
+}
+
+// outgoing directions of a closed face and their reflections, in the order and
+// with the first-match rule of m_boundary_{i,j,k}_closed_kernel.F90
+FacePairs face_pairs(int nl, int axis, int side, int opt) {
+    FacePairs fp;
+    memset(&fp, 0, sizeof(fp));
+    for (int l = 0; l < nl; ++l) {
+        int c[3] = {lat_cx(l), lat_cy(l), lat_cz(l)};
+        if (!((side == 0 && c[axis] < 0) || (side == 1 && c[axis] > 0))) continue;
+        int mv[3] = {opt * c[0], opt * c[1], opt * c[2]};
+        mv[axis] = -c[axis];
+        int m = lat_find(nl, mv[0], mv[1], mv[2]);
+        if (m < 0) continue;
+        fp.l[fp.n] = (int8_t)l;
+        fp.m[fp.n] = (int8_t)m;
+        fp.cx[fp.n] = (int8_t)c[0];
+        fp.cy[fp.n] = (int8_t)c[1];
+        fp.cz[fp.n] = (int8_t)c[2];
+        fp.n++;
+    }
+    return fp;
+}
+
+// one edge: ghost coords g (free axis -1), outgoing sign pattern s (0 = any),
+// mirror rule mr (component multipliers), pass-2 source coords src
+EdgeDesc edge_desc(int nl, const int g[3], const int s[3], const int mr[3], const int src[3]) {
+    EdgeDesc d;
+    memset(&d, 0, sizeof(d));
+    d.gi = g[0]; d.gj = g[1]; d.gk = g[2];
+    d.si = src[0]; d.sj = src[1]; d.sk = src[2];
+    for (int l = 0; l < nl; ++l) {
+        int c[3] = {lat_cx(l), lat_cy(l), lat_cz(l)};
+        bool out = true;
+        for (int a = 0; a < 3; ++a)
+            if (s[a] != 0 && c[a] * s[a] <= 0) out = false;
+        if (!out) continue;
+        int m = lat_find(nl, mr[0] * c[0], mr[1] * c[1], mr[2] * c[2]);
+        if (m < 0 || d.n >= 3) continue;
+        d.l[d.n] = (int8_t)l;
+        d.m[d.n] = (int8_t)m;
+        d.n++;
+    }
+    return d;
+}
+
+void setup_boundaries(lbm_ctx* c) {
+    const int nl = c->p.nl, nx = c->p.nx, ny = c->p.ny, nz = c->p.nz;
+    const int codes[3] = {c->p.ibnd, c->p.jbnd, c->p.kbnd};
+    for (int a = 0; a < 3; ++a) {
+        int o1, oN;
+        closed_opts(codes[a], o1, oN);
+        c->face_on[a] = (o1 != 0);
+        if (c->face_on[a]) {
+            c->face[a][0] = face_pairs(nl, a, 0, o1);
+            c->face[a][1] = face_pairs(nl, a, 1, oN);
+        }
+    }
+    const int ib = c->p.ibnd, jb = c->p.jbnd, kb = c->p.kbnd;
+    // j-k edges (m_boundary_j_k_edges.F90): free axis i; the (ny+1,nz+1) edge keeps cx (:129)
+    c->edges_on[0] = (jb > 10 && kb > 10);
+    if (c->edges_on[0]) {
+        const int opt = (jb == 22 && kb == 22) ? 1 : -1;
+        EdgeSet& es = c->edges[0];
+        es.free_axis = 0; es.nfree = nx; es.nedges = 4;
+        const int G[4][3] = {{-1, 0, 0}, {-1, ny + 1, 0}, {-1, 0, nz + 1}, {-1, ny + 1, nz + 1}};
+        const int S[4][3] = {{0, -1, -1}, {0, 1, -1}, {0, -1, 1}, {0, 1, 1}};
+        const int SRC[4][3] = {{-1, 1, 1}, {-1, ny, 1}, {-1, 1, nz}, {-1, ny, nz}};
+        for (int e = 0; e < 4; ++e) {
+            const int mr[3] = {e == 3 ? 1 : opt, -1, -1};
+            es.e[e] = edge_desc(nl, G[e], S[e], mr, SRC[e]);
+        }
+    }
+    // i-j edges (m_boundary_i_j_edges.F90): free axis k
+    c->edges_on[1] = (ib > 10 && jb > 10);
+    if (c->edges_on[1]) {
+        const int opt = (ib == 22 && jb == 22) ? 1 : -1;
+        EdgeSet& es = c->edges[1];
+        es.free_axis = 2; es.nfree = nz; es.nedges = 4;
+        const int G[4][3] = {{0, 0, -1}, {nx + 1, 0, -1}, {0, ny + 1, -1}, {nx + 1, ny + 1, -1}};
+        const int S[4][3] = {{-1, -1, 0}, {1, -1, 0}, {-1, 1, 0}, {1, 1, 0}};
+        const int SRC[4][3] = {{1, 1, -1}, {nx, 1, -1}, {1, ny, -1}, {nx, ny, -1}};
+        const int mr[3] = {-1, -1, opt};
+        for (int e = 0; e < 4; ++e) es.e[e] = edge_desc(nl, G[e], S[e], mr, SRC[e]);
+    }
+    // i-k edges (m_boundary_i_k_edges.F90): free axis j
+    c->edges_on[2] = (ib > 10 && kb > 10);
+    if (c->edges_on[2]) {
+        const int opt = (ib == 22 && kb == 22) ? 1 : -1;
+        EdgeSet& es = c->edges[2];
+        es.free_axis = 1; es.nfree = ny; es.nedges = 4;
+        const int G[4][3] = {{0, -1, 0}, {nx + 1, -1, 0}, {0, -1, nz + 1}, {nx + 1, -1, nz + 1}};
+        const int S[4][3] = {{-1, 0, -1}, {1, 0, -1}, {-1, 0, 1}, {1, 0, 1}};
+        const int SRC[4][3] = {{1, -1, 1}, {nx, -1, 1}, {1, -1, nz}, {nx, -1, nz}};
+        const int mr[3] = {-1, opt, -1};
+        for (int e = 0; e < 4; ++e) es.e[e] = edge_desc(nl, G[e], S[e], mr, SRC[e]);
+    }
+    // corners (m_boundary_closed_corners.F90), always no-slip
+    c->corners_on = (ib > 10 && jb > 10 && kb > 10);
+    if (c->corners_on) {
+        CornerSet& cs = c->corners;
+        int q = 0;
+        for (int ii = 0; ii < 2; ++ii)
+            for (int jj = 0; jj < 2; ++jj)
+                for (int kk = 0; kk < 2; ++kk, ++q) {
+                    cs.ci[q] = ii ? nx + 1 : 0;
+                    cs.cj[q] = jj ? ny + 1 : 0;
+                    cs.ck[q] = kk ? nz + 1 : 0;
+                    const int sx = ii ? 1 : -1, sy = jj ? 1 : -1, sz = kk ? 1 : -1;
+                    cs.l[q] = -1;
+                    cs.m[q] = -1;
+                    for (int l = 0; l < nl; ++l)
+                        if (lat_cx(l) * sx > 0 && lat_cy(l) * sy > 0 && lat_cz(l) * sz > 0) {
+                            cs.l[q] = l;
+                            cs.m[q] = lat_find(nl, -lat_cx(l), -lat_cy(l), -lat_cz(l));
+                            cs.cx[q] = (int8_t)lat_cx(l);
+                            cs.cy[q] = (int8_t)lat_cy(l);
+                            cs.cz[q] = (int8_t)lat_cz(l);
+                        }
+                }
+    }
+    // m_boundary_i_inflow_kernel.F90:191-193: cos(udir*pi/180), sin(udir*pi/180) in single precision
+    const float pi = 3.1415927410125732f;
+    c->cosd = cosf(c->p.udir * pi / 180.0f);
+    c->sind = sinf(c->p.udir * pi / 180.0f);
+}
+
+// boundarycond in the dispatch order of m_boundarycond.F90:14-468
+template <int Q, typename Acc>
+int run_bc(lbm_ctx* c, Acc f1, Acc f2, const float* uvel) {
+    const int nx = c->p.nx, ny = c->p.ny, nz = c->p.nz, nl = c->p.nl;
+    cudaStream_t s = c->stream;
+    auto periodic = [&](int axis) {
+        dim3 blk(128);
+        dim3 grd;
+        if (axis == 0) grd = dim3((ny + 2 + 127) / 128, nz + 2, nl);
+        else if (axis == 1) grd = dim3((nx + 2 + 127) / 128, nz + 2, nl);
+        else grd = dim3((nx + 2 + 127) / 128, ny + 2, nl);
+        k_periodic<Acc><<<grd, blk, 0, s>>>(f1, axis, nl);
+        c->launches++;
+    };
+    const int codes[3] = {c->p.ibnd, c->p.jbnd, c->p.kbnd};
+    for (int a = 0; a < 3; ++a)
+        if (codes[a] == 0) periodic(a);
+    for (int a = 0; a < 3; ++a) {
+        if (!c->face_on[a]) continue;
+        const int na = (a == 0) ? ny : nx;                  // first tangential extent
+        const int nb = (a == 2) ? ny : nz;                  // second tangential extent
+        dim3 grd((na + 127) / 128, nb, 2);
+        k_closed<Acc><<<grd, 128, 0, s>>>(f1, f2, a, c->face[a][0], c->face[a][1], 1, 1);
+        c->launches++;
+    }
+    for (int e = 0; e < 3; ++e) {
+        if (!c->edges_on[e]) continue;
+        const EdgeSet& es = c->edges[e];
+        k_edges<Acc><<<dim3((es.nfree + 127) / 128, 4), 128, 0, s>>>(f1, f2, es);
+        c->launches++;
+    }
+    if (c->corners_on) {
+        k_corners<Acc><<<1, 32, 0, s>>>(f1, f2, c->corners);
+        c->launches++;
+    }
+    if (c->p.ibnd == 1) {
+        k_inflow<Q, Acc><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(f1, uvel, c->p.rho0, c->cosd, c->sind);
+        c->launches++;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (codes[a] == 0) periodic(a);
+    LBM_LAUNCHED(c, "boundarycond");
+    return LBM_OK;
+}
+
+template <int Q>
+int bc_ref(lbm_ctx* c, float* f1, float* f2, const float* uvel) {
+    AosAcc a1{f1, c->rg}, a2{f2, c->rg};
+    return run_bc<Q>(c, a1, a2, uvel);
+}
+
+template <int Q, typename S>
+int bc_state(lbm_ctx* c, int i1, int i2) {
+    SoaAcc<S> a1{(S*)c->buf[i1], c->sg}, a2{(S*)c->buf[i2], c->sg};
+    return run_bc<Q>(c, a1, a2, c->d_uvel);
+}
+
+StepArgs step_args(lbm_ctx* c) {
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.g = c->sg;
+    a.cp = c->cp;
+    a.solid = c->d_solid;
+    if (c->nrturb > 0) {
+        const long long n = (long long)c->p.ny * c->p.nz * (c->nrturb + 1);
+        a.uu = c->d_turb;
+        a.vv = c->d_turb + n;
+        a.ww = c->d_turb + 2 * n;
+    }
+    a.nrturb = c->nrturb;
+    a.ampl = c->ampl;
+    a.iturb = c->p.iturb_pos;
+    a.d_it = c->d_it;
+    a.abl = c->d_abl;
+    a.status = c->d_status;
+    const long long g = c->rg.ncell();
+    a.rho_in = c->d_macro;
+    a.u_in = c->d_macro + g;
+    a.v_in = c->d_macro + 2 * g;
+    a.w_in = c->d_macro + 3 * g;
+    return a;
+}
+
+template <int Q, typename S>
+int step_one(lbm_ctx* c) {
+    const SoaGrid& g = c->sg;
+    dim3 grd((g.nx + 127) / 128, g.ny, g.nz);
+    StepArgs a = step_args(c);
+    if (c->state == ST_PRE) {
+        S* b = (S*)c->buf[c->cur];
+        k_step<Q, S, false><<<grd, 128, 0, c->stream>>>(b, b, a);
+        c->launches++;
+        LBM_LAUNCHED(c, "collide");
+        c->state = ST_POST;
+    } else {
+        const int nxt = 1 - c->cur;
+        LBM_TRY(prof_begin(c));
+        k_step<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        c->launches++;
+        LBM_LAUNCHED(c, "fused step");
+        LBM_TRY(prof_end(c));
+        c->cur = nxt;
+    }
+    LBM_TRY(bc_state<Q, S>(c, c->cur, 1 - c->cur));
+    k_bump_step<<<1, 32, 0, c->stream>>>(c->d_it);
+    c->launches++;
+    LBM_LAUNCHED(c, "step counter");
+    c->it += 1;
+    return LBM_OK;
+}
+
+int step_dispatch(lbm_ctx* c) {
+    const bool h = c->p.storage == LBM_STORE_F16;
+    if (c->p.nl == 27) return h ? step_one<27, __half>(c) : step_one<27, float>(c);
+    return h ? step_one<19, __half>(c) : step_one<19, float>(c);
+}
+
+template <int Q, typename S>
+void launch_import(lbm_ctx* c, const float* ref, int b) {
+    const SoaGrid& g = c->sg;
+    k_import<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(ref, (S*)c->buf[b], g);
+    c->launches++;
+}
+template <int Q, typename S>
+void launch_export(lbm_ctx* c, float* ref, int b, bool pull) {
+    const SoaGrid& g = c->sg;
+    dim3 grd((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2);
+    if (pull)
+        k_export<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], (const S*)c->buf[1 - b], ref, g);
+    else
+        k_export<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], nullptr, ref, g);
+    c->launches++;
+}
+template <int Q, typename S>
+void launch_macro(lbm_ctx* c, float* rho, float* u, float* v, float* w) {
+    const SoaGrid& g = c->sg;
+    k_macro<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(
+        (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g);
+    c->launches++;
+}
+
+#define DISPATCH_QS(c, FN, ...)                                                        \
+    do {                                                                               \
+        const bool _h = (c)->p.storage == LBM_STORE_F16;                               \
+        if ((c)->p.nl == 27) {                                                         \
+            if (_h) FN<27, __half>(__VA_ARGS__); else FN<27, float>(__VA_ARGS__);     \
+        } else {                                                                       \
+            if (_h) FN<19, __half>(__VA_ARGS__); else FN<19, float>(__VA_ARGS__);     \
+        }                                                                              \
+    } while (0)
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+int lbm_abi_version(void) { return LBM_B200_ABI_VERSION; }
+
+const char* lbm_last_error(const lbm_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int lbm_create(lbm_ctx** out, const lbm_params* p) {
+    if (!out || !p) return LBM_ERR_ARG;
+    *out = nullptr;
+    if (p->nl != 19 && p->nl != 27) return LBM_ERR_UNSUPPORTED;
+    if (p->nx < 2 || p->ny < 2 || p->nz < 2) return LBM_ERR_ARG;
+    if ((long long)(p->nx + 2) * (p->ny + 2) * (p->nz + 2) * p->nl >= (1LL << 40)) return LBM_ERR_ARG;
+    if (p->ibgk != 2 && p->ibgk != 3) return LBM_ERR_UNSUPPORTED;
+    if ((p->ihrr != 0 && p->ihrr != 1) || (p->ivreman != 0 && p->ivreman != 1)) return LBM_ERR_UNSUPPORTED;
+    if (p->storage != LBM_STORE_F32 && p->storage != LBM_STORE_F16) return LBM_ERR_UNSUPPORTED;
+    if (p->ibnd == 1 && (p->iturb_pos < 1 || p->iturb_pos > p->nx)) return LBM_ERR_ARG;
+    lbm_ctx* c = new lbm_ctx();
+    c->p = *p;
+    c->rg = RefGrid{p->nx, p->ny, p->nz, p->nl};
+    c->sg = SoaGrid::make(p->nx, p->ny, p->nz);
+    c->cp.kinevisc = p->kinevisc;
+    c->cp.cvre = 2.5f * p->smagorinsky * p->smagorinsky;
+    c->cp.eps = sqrtf(1.17549435e-38f);
+    c->cp.tau0 = 3.0f * p->kinevisc + 0.5f;
+    c->cp.ibgk = p->ibgk;
+    c->cp.ihrr = p->ihrr;
+    c->cp.ivreman = p->ivreman;
+    c->elem = (p->storage == LBM_STORE_F16) ? 2 : 4;
+    setup_boundaries(c);
+    int rc = LBM_OK;
+    auto chk = [&](cudaError_t e, const char* w) {
+        if (rc == LBM_OK && e != cudaSuccess) rc = cuda_check(c, e, w);
+    };
+    chk(cudaGetDevice(&c->dev), "cudaGetDevice");
+    c->stream = nullptr;
+    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem;
+    for (int b = 0; b < 2 && rc == LBM_OK; ++b) {
+        chk(cudaMalloc(&c->buf[b], nbuf), "cudaMalloc(state)");
+        if (rc == LBM_OK) chk(cudaMemset(c->buf[b], 0, nbuf), "cudaMemset(state)");
+    }
+    const size_t g = (size_t)c->rg.ncell();
+    chk(cudaMalloc(&c->d_macro, 4 * g * sizeof(float)), "cudaMalloc(macro)");
+    chk(cudaMalloc(&c->d_uvel, (size_t)p->nz * sizeof(float)), "cudaMalloc(uvel)");
+    chk(cudaMalloc(&c->d_abl, (size_t)p->nz * sizeof(float)), "cudaMalloc(ablvisc)");
+    chk(cudaMalloc(&c->d_it, 2 * sizeof(int)), "cudaMalloc(step)");
+    chk(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc(status)");
+    if (rc == LBM_OK) {
+        chk(cudaMemset(c->d_uvel, 0, (size_t)p->nz * sizeof(float)), "cudaMemset");
+        chk(cudaMemset(c->d_abl, 0, (size_t)p->nz * sizeof(float)), "cudaMemset");
+        chk(cudaMemset(c->d_it, 0, 2 * sizeof(int)), "cudaMemset");
+        chk(cudaMemset(c->d_status, 0, sizeof(int)), "cudaMemset");
+        chk(cudaDeviceSynchronize(), "create");
+    }
+    if (rc != LBM_OK) {
+        lbm_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_ctx* c) {
+    if (!c) return LBM_ERR_ARG;
+    cudaStreamSynchronize(c->stream);
+    for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
+    for (int b = 0; b < 2; ++b) cudaFree(c->buf[b]);
+    cudaFree(c->d_macro);
+    cudaFree(c->d_solid);
+    cudaFree(c->d_turb);
+    cudaFree(c->d_uvel);
+    cudaFree(c->d_abl);
+    cudaFree(c->d_it);
+    cudaFree(c->d_status);
+    delete c;
+    return LBM_OK;
+}
+
+int lbm_set_stream(lbm_ctx* c, void* stream) {
+    if (!c) return LBM_ERR_ARG;
+    c->stream = (cudaStream_t)stream;
+    return LBM_OK;
+}
+
+int lbm_synchronize(lbm_ctx* c) {
+    if (!c) return LBM_ERR_ARG;
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "synchronize");
+}
+
+// ---- per-call entry points ---------------------------------------------------
+
+int lbm_fequil3(lbm_ctx* c, float* feq, const float* rho, const float* u, const float* v, const float* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, feq); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_fequil3<27><<<grd, 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
+    else k_ref_fequil3<19><<<grd, 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
+    c->launches++;
+    LBM_LAUNCHED(c, "fequil3");
+    return LBM_OK;
+}
+
+int lbm_postcoll(lbm_ctx* c, float* f, float* tau, const float* rho, const float* u, const float* v, const float* w,
+                 const float* ablvisc) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, tau); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_postcoll<27><<<grd, 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, c->cp);
+    else k_ref_postcoll<19><<<grd, 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, c->cp);
+    c->launches++;
+    LBM_LAUNCHED(c, "postcoll");
+    return LBM_OK;
+}
+
+int lbm_drift(lbm_ctx* c, float* f, const float* feq) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq);
+    if (f == feq) return fail(c, LBM_ERR_ARG, "drift: f and feq must be distinct buffers");
+    dim3 grd((c->p.nl * c->p.nx + 255) / 256, c->p.ny, c->p.nz);
+    k_ref_drift<<<grd, 256, 0, c->stream>>>(f, feq, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "drift");
+    return LBM_OK;
+}
+
+int lbm_macrovars(lbm_ctx* c, float* rho, float* u, float* v, float* w, const float* f) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, f);
+    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
+    if (c->p.nl == 27) k_ref_macrovars<27><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
+    else k_ref_macrovars<19><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "macrovars");
+    return LBM_OK;
+}
+
+int lbm_regularization(lbm_ctx* c, float* f, const float* feq, const float* u, const float* v, const float* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq); NEED(c, u); NEED(c, v); NEED(c, w);
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_regularization<27><<<grd, 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
+    else k_ref_regularization<19><<<grd, 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "regularization");
+    return LBM_OK;
+}
+
+int lbm_vreman(lbm_ctx* c, const float* f, float* tau) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, tau);
+    if (c->p.ivreman != 1) return LBM_OK;   // m_vreman.F90:211-213
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_vreman<27><<<grd, 128, 0, c->stream>>>(f, tau, c->rg, c->cp);
+    else k_ref_vreman<19><<<grd, 128, 0, c->stream>>>(f, tau, c->rg, c->cp);
+    c->launches++;
+    LBM_LAUNCHED(c, "vreman");
+    return LBM_OK;
+}
+
+static int axpy(lbm_ctx* c, float* f, const float* feq, float sgn, const char* what) {
+    NEED(c, f); NEED(c, feq);
+    const long long n = c->rg.ncell() * c->p.nl;
+    k_ref_axpy<<<148 * 8, 256, 0, c->stream>>>(f, feq, n, sgn);
+    c->launches++;
+    LBM_LAUNCHED(c, what);
+    return LBM_OK;
+}
+int lbm_compute_fneq(lbm_ctx* c, float* f, const float* feq) {
+    if (!c) return LBM_ERR_ARG;
+    return axpy(c, f, feq, -1.f, "compute_fneq");
+}
+int lbm_compute_f(lbm_ctx* c, float* f, const float* feq) {
+    if (!c) return LBM_ERR_ARG;
+    return axpy(c, f, feq, 1.f, "compute_f");
+}
+
+int lbm_boundarycond(lbm_ctx* c, float* f1, float* f2, const float* uvel) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f1); NEED(c, f2);
+    if (c->p.ibnd == 1) NEED(c, uvel);
+    if (f1 == f2) return fail(c, LBM_ERR_ARG, "boundarycond: f1 and f2 must be distinct buffers");
+    return c->p.nl == 27 ? bc_ref<27>(c, f1, f2, uvel) : bc_ref<19>(c, f1, f2, uvel);
+}
+
+int lbm_solids(lbm_ctx* c, float* f, const int32_t* blanking) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, blanking);
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_solids<27><<<grd, 128, 0, c->stream>>>(f, blanking, c->rg);
+    else k_ref_solids<19><<<grd, 128, 0, c->stream>>>(f, blanking, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "solids");
+    return LBM_OK;
+}
+
+int lbm_inflow_turbulence_forcing(lbm_ctx* c, float* df, const float* rho, const float* u, const float* v,
+                                  const float* w, const float* uu, const float* vv, const float* ww, float ampl,
+                                  int32_t it, int32_t nrturb) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, df); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, uu); NEED(c, vv); NEED(c, ww);
+    if (nrturb <= 0) return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: nrturb must be positive");
+    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
+        return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: iturb_pos outside 1..nx");
+    int lit = it % nrturb;   // m_inflow_turbulence_forcing.F90:45-46
+    if (lit < 0) lit += nrturb;
+    if (lit == 0) lit = nrturb;
+    dim3 grd((c->p.ny + 127) / 128, c->p.nz);
+    if (c->p.nl == 27)
+        k_ref_turb_forcing<27><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
+                                                           c->p.ibgk, c->rg);
+    else
+        k_ref_turb_forcing<19><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
+                                                           c->p.ibgk, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "inflow_turbulence_forcing");
+    return LBM_OK;
+}
+
+int lbm_inflow_turbulence_apply(lbm_ctx* c, float* f, const float* df) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, df);
+    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
+        return fail(c, LBM_ERR_ARG, "inflow_turbulence_apply: iturb_pos outside 1..nx");
+    dim3 grd((c->p.nl * c->p.ny + 255) / 256, c->p.nz);
+    k_ref_turb_apply<<<grd, 256, 0, c->stream>>>(f, df, c->p.iturb_pos, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "inflow_turbulence_apply");
+    return LBM_OK;
+}
+
+int lbm_fillghosts(lbm_ctx* c, float* f) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f);
+    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
+    k_ref_fillghosts<<<grd, 128, 0, c->stream>>>(f, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "fillghosts");
+    return LBM_OK;
+}
+
+// ---- fused state API -----------------------------------------------------------
+
+int lbm_state_import(lbm_ctx* c, const float* f1, const float* f2, const float* rho, const float* u, const float* v,
+                     const float* w, int32_t it) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f1); NEED(c, f2); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    DISPATCH_QS(c, launch_import, c, f1, 0);
+    DISPATCH_QS(c, launch_import, c, f2, 1);
+    const size_t g = (size_t)c->rg.ncell() * sizeof(float);
+    const float* src[4] = {rho, u, v, w};
+    for (int q = 0; q < 4; ++q)
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync((char*)c->d_macro + q * g, src[q], g, cudaMemcpyDeviceToDevice, c->stream),
+                           "import macro"));
+    const int nxt = it + 1;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_it, &nxt, sizeof(int), cudaMemcpyHostToDevice, c->stream), "import step"));
+    LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "import"));
+    LBM_LAUNCHED(c, "import");
+    c->cur = 0;
+    c->it = it;
+    c->state = ST_PRE;
+    return LBM_OK;
+}
+
+int lbm_state_export(lbm_ctx* c, float* f1, float* f2) {
+    if (!c) return LBM_ERR_ARG;
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "state_export: no state imported");
+    NEED(c, f1); NEED(c, f2);
+    const bool post = (c->state == ST_POST);
+    if (post) {
+        DISPATCH_QS(c, launch_export, c, f1, c->cur, true);
+        DISPATCH_QS(c, launch_export, c, f2, c->cur, false);
+    } else {
+        DISPATCH_QS(c, launch_export, c, f1, c->cur, false);
+        DISPATCH_QS(c, launch_export, c, f2, 1 - c->cur, false);
+    }
+    LBM_LAUNCHED(c, "export");
+    return LBM_OK;
+}
+
+int lbm_get_macro(lbm_ctx* c, float* rho, float* u, float* v, float* w) {
+    if (!c) return LBM_ERR_ARG;
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "get_macro: no state imported");
+    NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    if (c->state == ST_PRE) {
+        const size_t g = (size_t)c->rg.ncell() * sizeof(float);
+        float* dst[4] = {rho, u, v, w};
+        for (int q = 0; q < 4; ++q)
+            LBM_TRY(cuda_check(c, cudaMemcpyAsync(dst[q], (char*)c->d_macro + q * g, g, cudaMemcpyDeviceToDevice,
+                                                  c->stream), "get_macro"));
+        return LBM_OK;
+    }
+    DISPATCH_QS(c, launch_macro, c, rho, u, v, w);
+    LBM_LAUNCHED(c, "get_macro");
+    return LBM_OK;
+}
+
+__global__ void k_mask_from_logical(uint8_t* m, const int32_t* blank, RefGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    m[((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)] = blank[g.cell(i, j, k)] != 0;
+}
+
+int lbm_set_solids(lbm_ctx* c, const int32_t* blanking) {
+    if (!c) return LBM_ERR_ARG;
+    if (!blanking) {
+        LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "set_solids"));
+        cudaFree(c->d_solid);
+        c->d_solid = nullptr;
+        return LBM_OK;
+    }
+    if (!c->d_solid)
+        LBM_TRY(cuda_check(c, cudaMalloc(&c->d_solid, (size_t)c->p.nx * c->p.ny * c->p.nz), "cudaMalloc(solids)"));
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    k_mask_from_logical<<<grd, 128, 0, c->stream>>>(c->d_solid, blanking, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "set_solids");
+    return LBM_OK;
+}
+
+int lbm_set_turbulence(lbm_ctx* c, const float* uu, const float* vv, const float* ww, int32_t nrturb, float ampl) {
+    if (!c) return LBM_ERR_ARG;
+    if (!uu) {
+        LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "set_turbulence"));
+        cudaFree(c->d_turb);
+        c->d_turb = nullptr;
+        c->nrturb = 0;
+        return LBM_OK;
+    }
+    NEED(c, vv); NEED(c, ww);
+    if (nrturb <= 0) return fail(c, LBM_ERR_ARG, "set_turbulence: nrturb must be positive");
+    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
+        return fail(c, LBM_ERR_ARG, "set_turbulence: iturb_pos outside 1..nx");
+    const size_t n = (size_t)c->p.ny * c->p.nz * (nrturb + 1);
+    LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "set_turbulence"));
+    cudaFree(c->d_turb);
+    c->d_turb = nullptr;
+    LBM_TRY(cuda_check(c, cudaMalloc(&c->d_turb, 3 * n * sizeof(float)), "cudaMalloc(turbulence)"));
+    const float* src[3] = {uu, vv, ww};
+    for (int q = 0; q < 3; ++q)
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_turb + q * n, src[q], n * sizeof(float), cudaMemcpyDeviceToDevice,
+                                              c->stream), "set_turbulence"));
+    c->nrturb = nrturb;
+    c->ampl = ampl;
+    return LBM_OK;
+}
+
+int lbm_set_inflow(lbm_ctx* c, const float* uvel) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, uvel);
+    return cuda_check(c, cudaMemcpyAsync(c->d_uvel, uvel, (size_t)c->p.nz * sizeof(float), cudaMemcpyDeviceToDevice,
+                                         c->stream), "set_inflow");
+}
+
+int lbm_step(lbm_ctx* c, int32_t nsteps) {
+    if (!c) return LBM_ERR_ARG;
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "step: no state imported");
+    if (nsteps < 0) return fail(c, LBM_ERR_ARG, "step: nsteps < 0");
+    for (int s = 0; s < nsteps; ++s) LBM_TRY(step_dispatch(c));
+    return LBM_OK;
+}
+
+int lbm_step_host(lbm_ctx* c, int32_t nsteps, const float* uvel_host, int32_t* status_host) {
+    if (!c) return LBM_ERR_ARG;
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "step_host: no state imported");
+    if (nsteps < 0) return fail(c, LBM_ERR_ARG, "step_host: nsteps < 0");
+    for (int s = 0; s < nsteps; ++s) {
+        if (uvel_host)
+            LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_uvel, uvel_host, (size_t)c->p.nz * sizeof(float),
+                                                  cudaMemcpyHostToDevice, c->stream), "step_host uvel"));
+        LBM_TRY(step_dispatch(c));
+    }
+    if (status_host) {
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(status_host, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream),
+                           "step_host status"));
+        LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "step_host"));
+    }
+    return LBM_OK;
+}
+
+int lbm_get_step(lbm_ctx* c, int32_t* it) {
+    if (!c || !it) return LBM_ERR_ARG;
+    *it = c->it;
+    return LBM_OK;
+}
+
+int lbm_launch_count(lbm_ctx* c, int64_t* n) {
+    if (!c || !n) return LBM_ERR_ARG;
+    *n = c->launches;
+    return LBM_OK;
+}
+
+int lbm_profile(lbm_ctx* c, int32_t enable) {
+    if (!c) return LBM_ERR_ARG;
+    if (enable && c->ev.empty()) {
+        c->ev.resize(2 * 1024);
+        for (auto& e : c->ev) LBM_TRY(cuda_check(c, cudaEventCreate(&e), "cudaEventCreate"));
+    }
+    LBM_TRY(prof_drain(c));
+    c->profiling = enable != 0;
+    c->prof_ms = 0.0;
+    c->prof_launches = 0;
+    return LBM_OK;
+}
+
+int lbm_profile_read(lbm_ctx* c, double* step_kernel_ms, int64_t* step_kernel_launches) {
+    if (!c || !step_kernel_ms || !step_kernel_launches) return LBM_ERR_ARG;
+    LBM_TRY(prof_drain(c));
+    *step_kernel_ms = c->prof_ms;
+    *step_kernel_launches = c->prof_launches;
+    return LBM_OK;
+}
+
+int lbm_status(lbm_ctx* c, int32_t* flags) {
+    if (!c || !flags) return LBM_ERR_ARG;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(flags, c->d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status"));
+    LBM_TRY(cuda_check(c, cudaMemsetAsync(c->d_status, 0, sizeof(int), c->stream), "status"));
+    LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "status"));
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// common.cuh -- lattice tables, grid layouts and storage traits shared by the
+// kernels of the B200 LBM library.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lbm {
+
+// ---------------------------------------------------------------------------
+// Lattice tables in the reference's direction order (mod_D3Q27setup.F90:28-48).
+// D3Q19 is the first 19 directions of D3Q27.  Directions 2k-1 and 2k
+// (0-based, k >= 1) are opposite, which both the solid swap (m_solids.F90:28-32)
+// and the pairwise evaluation of the collision rely on.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int lat_cx(int l) {
+    constexpr int t[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1};
+    return t[l];
+}
+__host__ __device__ constexpr int lat_cy(int l) {
+    constexpr int t[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 0, 0, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+    return t[l];
+}
+__host__ __device__ constexpr int lat_cz(int l) {
+    constexpr int t[27] = {0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1};
+    return t[l];
+}
+__host__ __device__ constexpr int lat_speed2(int l) {
+    return lat_cx(l) * lat_cx(l) + lat_cy(l) * lat_cy(l) + lat_cz(l) * lat_cz(l);
+}
+// weights: D3Q19 {1/3, 1/18, 1/36}; D3Q27 {8/27, 2/27, 1/54, 1/216}
+template <int Q>
+__host__ __device__ constexpr float lat_w(int l) {
+    return Q == 19 ? (lat_speed2(l) == 0 ? 1.0f / 3.0f : lat_speed2(l) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f)
+                   : (lat_speed2(l) == 0 ? 8.0f / 27.0f
+                      : lat_speed2(l) == 1 ? 2.0f / 27.0f
+                      : lat_speed2(l) == 2 ? 1.0f / 54.0f
+                                           : 1.0f / 216.0f);
+}
+__host__ __device__ constexpr int lat_opposite(int l) { return l == 0 ? 0 : ((l & 1) ? l + 1 : l - 1); }
+
+// ---------------------------------------------------------------------------
+// Reference layout f(nl,0:nx+1,0:ny+1,0:nz+1), l fastest (Fortran column-major).
+// ---------------------------------------------------------------------------
+struct RefGrid {
+    int nx, ny, nz, nl;
+    __host__ __device__ long long cell(int i, int j, int k) const {
+        return (long long)i + (long long)(nx + 2) * ((long long)j + (long long)(ny + 2) * k);
+    }
+    __host__ __device__ long long ncell() const { return (long long)(nx + 2) * (ny + 2) * (nz + 2); }
+};
+
+// ---------------------------------------------------------------------------
+// Structure-of-arrays layout of the fused state.  Each direction is a block of
+// (ny+2)*(nz+2) rows of `pitch` elements; in a row, ghost i=0 sits at offset
+// 31 so that the interior i=1..nx starts on a 128-byte boundary (FP32) and a
+// warp of consecutive i writes whole cache lines.  pitch = roundup(nx+2, 32)
+// leaves room for ghost nx+1 before the next row's ghost 0.
+// ---------------------------------------------------------------------------
+struct SoaGrid {
+    int nx, ny, nz;
+    int pitch;            // elements per row
+    long long rowsz;      // elements per (j,k) row block = pitch
+    long long dstride;    // elements per direction
+    __host__ __device__ int row(int j, int k) const { return k * (ny + 2) + j; }
+    // element offset of cell (i,j,k) inside a direction block (i,j,k ghost-inclusive)
+    __host__ __device__ long long off(int i, int j, int k) const {
+        return (long long)row(j, k) * pitch + 31 + i;
+    }
+    static SoaGrid make(int nx, int ny, int nz) {
+        SoaGrid g;
+        g.nx = nx; g.ny = ny; g.nz = nz;
+        g.pitch = ((nx + 2 + 31) / 32) * 32;
+        g.rowsz = g.pitch;
+        g.dstride = (long long)(ny + 2) * (nz + 2) * g.pitch + 32;
+        return g;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Storage traits: the fused state stores f' = f - w_l, the offset from the
+// rest-state weight, either in FP32 or as FP16 scaled by 2^8.  The offset
+// form keeps the small non-equilibrium part away from the large constant w_l,
+// which costs nothing in FP32 and is what makes FP16 storage usable.
+// ---------------------------------------------------------------------------
+template <typename S>
+struct Store;
+template <>
+struct Store<float> {
+    static __device__ __forceinline__ float load(const float* p) { return __ldg(p); }
+    static __device__ __forceinline__ void store(float* p, float v) { *p = v; }
+    static __host__ __device__ __forceinline__ float to_f(float s) { return s; }
+    static __host__ __device__ __forceinline__ float from_f(float v) { return v; }
+};
+template <>
+struct Store<__half> {
+    static __device__ __forceinline__ float load(const __half* p) { return __half2float(__ldg(p)) * (1.0f / 256.0f); }
+    static __device__ __forceinline__ void store(__half* p, float v) { *p = __float2half_rn(v * 256.0f); }
+    static __device__ __forceinline__ float to_f(__half s) { return __half2float(s) * (1.0f / 256.0f); }
+    static __device__ __forceinline__ __half from_f(float v) { return __float2half_rn(v * 256.0f); }
+};
+
+}  // namespace lbm

@@ -1,0 +1,316 @@
+// ref_kernels.cuh -- per-call kernels on the reference layout
+// f(nl,0:nx+1,0:ny+1,0:nz+1) (l fastest), one per reference subroutine.
+//
+// Cell-wise kernels stage a row chunk of 128 cells (128*nl contiguous floats)
+// through shared memory, so the global reads and writes are coalesced even
+// though each cell's nl populations are contiguous; the per-cell math reads
+// the staged values with an odd stride (nl = 19 or 27), free of bank
+// conflicts.
+#pragma once
+
+#include "collide.cuh"
+
+namespace lbm {
+
+__constant__ int8_t c_cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1};
+__constant__ int8_t c_cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 0, 0, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+__constant__ int8_t c_cz[27] = {0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1};
+
+// Equilibrium offsets feq_l - w_l (m_fequil3_kernel.F90:112-167 in closed form).
+template <int Q>
+__device__ __forceinline__ void equilibrium(float (&fe)[Q], float drho, float rho, float ux, float uy, float uz,
+                                            bool cubic) {
+    const float usq = ux * ux + uy * uy + uz * uz;
+    const float R45 = 4.5f * rho;
+    const float R45o = cubic ? R45 : 0.0f;
+    const float A0 = drho - 1.5f * rho * usq;
+    const float B0 = 3.0f * rho - (cubic ? R45 * usq : 0.0f);
+    fe[0] = lat_w<Q>(0) * A0;
+#pragma unroll
+    for (int l = 1; l < Q; l += 2) {
+        const float w = lat_w<Q>(l);
+        const float cu = cdot(lat_cx(l), lat_cy(l), lat_cz(l), ux, uy, uz);
+        const float cu2 = cu * cu;
+        const float E = w * (A0 + R45 * cu2);
+        const float O = w * cu * (B0 + R45o * cu2);
+        fe[l] = E + O;
+        fe[l + 1] = E - O;
+    }
+}
+
+// Regularized non-equilibrium R(fneq) from a2 = sum H2 fneq (all l, including rest).
+template <int Q>
+__device__ __forceinline__ void regularized(float (&out)[Q], const Moments& m, float ux, float uy, float uz) {
+    const float third = 1.0f / 3.0f;
+    const float axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
+    const float axy = m.pxy, axz = m.pxz, ayz = m.pyz;
+    const float tr = axx + ayy + azz;
+    const float vx = axx * ux + axy * uy + axz * uz;
+    const float vy = axy * ux + ayy * uy + ayz * uz;
+    const float vz = axz * ux + ayz * uy + azz * uz;
+    out[0] = lat_w<Q>(0) * 4.5f * (-tr * third);
+#pragma unroll
+    for (int l = 1; l < Q; l += 2) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        const float w = 4.5f * lat_w<Q>(l);
+        const float cu = cdot(cx, cy, cz, ux, uy, uz);
+        float cac = 0.f;
+        macc(cac, cx * cx, axx);
+        macc(cac, cy * cy, ayy);
+        macc(cac, cz * cz, azz);
+        macc(cac, cx * cy, 2.0f * axy);
+        macc(cac, cx * cz, 2.0f * axz);
+        macc(cac, cy * cz, 2.0f * ayz);
+        const float cau = cdot(cx, cy, cz, vx, vy, vz);
+        const float E = w * (cac - tr * third);
+        const float O = w * (cu * (3.0f * cac - tr) - 2.0f * cau);
+        out[l] = E + O;
+        out[l + 1] = E - O;
+    }
+}
+
+// Row-chunk staging: cells [i0, i0+n) of row (j,k), n <= 128.
+template <int Q>
+__device__ __forceinline__ void tile_load(float* sm, const float* f, long long cell0, int n) {
+    const long long base = cell0 * Q;
+    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) sm[e] = f[base + e];
+}
+template <int Q>
+__device__ __forceinline__ void tile_store(const float* sm, float* f, long long cell0, int n) {
+    const long long base = cell0 * Q;
+    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) f[base + e] = sm[e];
+}
+
+// fequil3: feq on interior cells (m_fequil3_kernel.F90:7-123)
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_fequil3(float* feq, const float* rho, const float* u, const float* v,
+                                                     const float* w, RefGrid g, int ibgk) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        float fe[Q];
+        equilibrium<Q>(fe, rho[c] - 1.0f, rho[c], u[c], v[c], w[c], ibgk == 3);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fe[l] + lat_w<Q>(l);
+    }
+    __syncthreads();
+    tile_store<Q>(sm, feq, g.cell(i0, j, k), n);
+}
+
+// postcoll: collide interior cells in place with the given moments (m_postcoll_kernel.F90:7-255)
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, const float* rho, const float* u,
+                                                      const float* v, const float* w, const float* abl, RefGrid g,
+                                                      CollideParams cp) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sm, f, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        float fp[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fp[l] = sm[t * Q + l] - lat_w<Q>(l);
+        const Moments m = moments<Q>(fp);
+        const float r = rho[c];
+        TurbIn tb;
+        tb.on = false;
+        tb.dux = tb.duy = tb.duz = 0.f;
+        const float tnew = collide<Q>(fp, m, r - 1.0f, r, u[c], v[c], w[c], cp, abl ? abl[k - 1] : 0.0f, tau[c],
+                                      false, tb);
+        if (cp.ivreman) tau[c] = tnew;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fp[l] + lat_w<Q>(l);
+    }
+    __syncthreads();
+    tile_store<Q>(sm, f, g.cell(i0, j, k), n);
+}
+
+// drift: f(l,i,j,k) = feq(l,i-cx,j-cy,k-cz) over interior cells; a thread per
+// (l,i) of a row, as m_drift_kernel.F90:62-84 flattens it
+__global__ void k_ref_drift(float* f, const float* feq, RefGrid g) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int nl = g.nl;
+    if (idx >= nl * g.nx) return;
+    const int l = idx % nl, i = idx / nl + 1;
+    f[g.cell(i, j, k) * nl + l] = feq[g.cell(i - c_cx[l], j - c_cy[l], k - c_cz[l]) * nl + l];
+}
+
+// macrovars over the ghost-inclusive grid, summation order of m_macrovars_kernel.F90:175-187
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_macrovars(float* rho, float* u, float* v, float* w, const float* f,
+                                                       RefGrid g) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128, j = blockIdx.y, k = blockIdx.z;
+    const int n = min(128, g.nx + 2 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sm, f, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        float tr = 0.f, tu = 0.f, tv = 0.f, tw = 0.f;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            const float tf = sm[t * Q + l];
+            tr = tr + tf;
+            macc(tu, lat_cx(l), tf);
+            macc(tv, lat_cy(l), tf);
+            macc(tw, lat_cz(l), tf);
+        }
+        const float inv = 1.0f / tr;
+        const long long c = g.cell(i0 + t, j, k);
+        rho[c] = tr;
+        u[c] = tu * inv;
+        v[c] = tv * inv;
+        w[c] = tw * inv;
+    }
+}
+
+// regularization: f = R(f - feq) on interior cells (m_regularization_kernel.F90:6-122)
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_regularization(float* f, const float* feq, const float* u,
+                                                            const float* v, const float* w, RefGrid g) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sm, f, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        float fn[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fn[l] = sm[t * Q + l] - feq[c * Q + l];
+        const Moments m = moments<Q>(fn);
+        float out[Q];
+        regularized<Q>(out, m, u[c], v[c], w[c]);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = out[l];
+    }
+    __syncthreads();
+    tile_store<Q>(sm, f, g.cell(i0, j, k), n);
+}
+
+// vreman: tau from a non-equilibrium f with the standalone guards
+// (alphamag and beta start at 1e-5, no ablvisc; m_vreman_kernel.F90:281-325)
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_vreman(const float* f, float* tau, RefGrid g, CollideParams cp) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sm, f, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        float fn[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fn[l] = sm[t * Q + l];
+        const Moments m = moments<Q>(fn);
+        const float third = 1.0f / 3.0f;
+        const float axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
+        const float axy = m.pxy, axz = m.pxz, ayz = m.pyz;
+        const float g0 = 0.00001f;
+        const float amag = g0 + (axx * axx + ayy * ayy + azz * azz + 2.0f * (axy * axy + axz * axz + ayz * ayz));
+        const float b11 = g0 + axx * axx + axy * axy + axz * axz;
+        const float b22 = g0 + axy * axy + ayy * ayy + ayz * ayz;
+        const float b33 = g0 + axz * axz + ayz * ayz + azz * azz;
+        const float b12 = g0 + axx * axy + axy * ayy + axz * ayz;
+        const float b13 = g0 + axx * axz + axy * ayz + axz * azz;
+        const float b23 = g0 + axy * axz + ayy * ayz + ayz * azz;
+        const float bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+        const float tt = bb / amag;
+        const float nut = (tt > cp.eps) ? cp.cvre * sqrtf(tt) : 0.0f;
+        tau[g.cell(i0 + t, j, k)] = 3.0f * (cp.kinevisc + nut) + 0.5f;
+    }
+}
+
+// compute_fneq / compute_f: elementwise over every element, ghosts included
+__global__ void k_ref_axpy(float* f, const float* feq, long long n, float sgn) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        f[e] = (sgn > 0.f) ? (feq[e] + f[e]) : (f[e] - feq[e]);
+}
+
+// solids: swap pairs (l,l+1), l = 2,4,..,nl-1 (1-based) at blanked interior cells (m_solids.F90:24-36)
+template <int Q>
+__global__ void k_ref_solids(float* f, const int32_t* blank, RefGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    const long long c = g.cell(i, j, k);
+    if (blank[c] == 0) return;
+    float* p = f + c * Q;
+#pragma unroll
+    for (int l = 1; l + 1 < Q; l += 2) {
+        const float a = p[l];
+        p[l] = p[l + 1];
+        p[l + 1] = a;
+    }
+}
+
+// inflow_turbulence_forcing: df(l,j,k) = feq(rho,u+ampl*uu) - feq(rho,u) at i = iturb
+// (m_inflow_turbulence_forcing.F90:44-128), evaluated as a difference of offsets
+template <int Q>
+__global__ void k_ref_turb_forcing(float* df, const float* rho, const float* u, const float* v, const float* w,
+                                   const float* uu, const float* vv, const float* ww, float ampl, int lit, int ip,
+                                   int ibgk, RefGrid g) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
+    if (j > g.ny) return;
+    const long long c = g.cell(ip, j, k);
+    const long long t = (long long)(j - 1) + (long long)g.ny * ((long long)(k - 1) + (long long)g.nz * lit);
+    const float r = rho[c];
+    const float ux = u[c], uy = v[c], uz = w[c];
+    const float dux = ampl * uu[t], duy = ampl * vv[t], duz = ampl * ww[t];
+    const bool cubic = ibgk == 3;
+    const float usq = ux * ux + uy * uy + uz * uz;
+    const float dusq = dux * (2.0f * ux + dux) + duy * (2.0f * uy + duy) + duz * (2.0f * uz + duz);
+    const float usq2 = usq + dusq;
+    float* o = df + ((long long)(j - 1) + (long long)g.ny * (k - 1)) * Q;
+    o[0] = lat_w<Q>(0) * r * (-1.5f * dusq);
+#pragma unroll
+    for (int l = 1; l < Q; l += 2) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        const float wr = lat_w<Q>(l) * r;
+        const float cu = cdot(cx, cy, cz, ux, uy, uz);
+        const float dcu = cdot(cx, cy, cz, dux, duy, duz);
+        const float cun = cu + dcu;
+        const float E = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
+        float od = 3.0f * dcu;
+        if (cubic) od += 4.5f * dcu * (cun * cun + cun * cu + cu * cu - usq2) - 4.5f * cu * dusq;
+        const float O = wr * od;
+        o[l] = E + O;
+        o[l + 1] = E - O;
+    }
+}
+
+// inflow_turbulence_apply: f(l,ip,j,k) += df(l,j,k) (m_inflow_turbulence_apply.F90:19-28)
+__global__ void k_ref_turb_apply(float* f, const float* df, int ip, RefGrid g) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;   // over (l, j)
+    const int k = blockIdx.y + 1;
+    const int nl = g.nl;
+    if (e >= nl * g.ny) return;
+    const int l = e % nl, j = e / nl + 1;
+    f[g.cell(ip, j, k) * nl + l] += df[((long long)(j - 1) + (long long)g.ny * (k - 1)) * nl + l];
+}
+
+// fillghosts: ghost cells copy the nearest interior cell (m_fillghosts.F90:18-29)
+__global__ void k_ref_fillghosts(float* f, RefGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i > g.nx + 1) return;
+    const int i1 = min(max(i, 1), g.nx), j1 = min(max(j, 1), g.ny), k1 = min(max(k, 1), g.nz);
+    if (i1 == i && j1 == j && k1 == k) return;
+    const int nl = g.nl;
+    const float* s = f + g.cell(i1, j1, k1) * nl;
+    float* d = f + g.cell(i, j, k) * nl;
+    for (int l = 0; l < nl; ++l) d[l] = s[l];
+}
+
+}  // namespace lbm

@@ -1,0 +1,91 @@
+"""The C ABI library loads and exports every symbol include/lbm_b200.h declares
+(no compute calls: these run without a GPU)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from lbm_b200 import _lib, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "lbm_b200.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(lbm_\w+)\s*\(", txt, flags=re.M)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return _lib.load()
+
+
+def test_header_parses():
+    names = header_functions()
+    assert "lbm_postcoll" in names and "lbm_step" in names and "lbm_boundarycond" in names
+    assert len(names) >= 29
+
+
+def test_library_exports_every_header_symbol(lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = set(re.findall(r"\sT\s(\w+)$", out.stdout, flags=re.M))
+    missing = [n for n in header_functions() if n not in exported]
+    assert not missing, "not exported: %s" % missing
+    for n in header_functions():
+        assert hasattr(lib, n)
+
+
+def test_bindings_cover_header():
+    bound = set(_lib.SIGNATURES) | {"lbm_last_error"}
+    assert set(header_functions()) == bound
+
+
+def test_library_does_not_link_the_oracle(lib):
+    out = subprocess.run(["nm", "-D", _lib.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    assert "orc_" not in out
+    ldd = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    assert "oracle" not in ldd
+
+
+def test_abi_version(lib):
+    assert lib.lbm_abi_version() == 1
+
+
+def test_params_struct_matches_header():
+    txt = open(HEADER).read()
+    body = re.search(r"typedef struct lbm_params \{(.*?)\} lbm_params;", txt, flags=re.S).group(1)
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = []
+    for decl in body.split(";"):
+        decl = decl.strip()
+        if not decl:
+            continue
+        ty, names = decl.split(None, 1)
+        fields += [(n.strip(), ty) for n in names.split(",")]
+    py = [(n, t) for n, t in _lib.LbmParams._fields_]
+    assert [n for n, _ in fields] == [n for n, _ in py]
+    for (n, ty), (_, ct) in zip(fields, py):
+        assert (ty == "float") == (ct is ctypes.c_float), n
+    assert ctypes.sizeof(_lib.LbmParams) == 4 * len(fields)
+
+
+def test_null_context_is_an_error_not_a_crash(lib):
+    assert lib.lbm_step(None, 1) == _lib.LBM_ERR_ARG
+    assert lib.lbm_destroy(None) == _lib.LBM_ERR_ARG
+    assert lib.lbm_postcoll(None, None, None, None, None, None, None, None) == _lib.LBM_ERR_ARG
+
+
+def test_create_rejects_bad_params_before_touching_the_gpu(lib):
+    h = ctypes.c_void_p()
+    for bad in (dict(nl=15), dict(nx=1), dict(ibgk=4), dict(storage=7), dict(ihrr=2)):
+        kw = dict(nx=8, ny=8, nz=8, nl=27, ibgk=3, ihrr=1, ivreman=1, ibnd=1, jbnd=0, kbnd=12,
+                  iturb_pos=3, storage=0, kinevisc=1e-4, smagorinsky=0.15, rho0=1.0, udir=0.0)
+        kw.update(bad)
+        p = _lib.LbmParams(**kw)
+        rc = lib.lbm_create(ctypes.byref(h), ctypes.byref(p))
+        assert rc in (_lib.LBM_ERR_ARG, _lib.LBM_ERR_UNSUPPORTED), (bad, rc)
