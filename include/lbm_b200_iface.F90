@@ -1,0 +1,165 @@
+! lbm_b200_iface.F90 -- Fortran 2003 ISO_C_BINDING interface to liblbmb200.so.
+!
+! Mirrors include/lbm_b200.h.  Every array argument is a device address passed
+! by value as type(c_ptr); with nvfortran obtain it with c_devloc() from the
+! cudafor module, e.g.  ierr = lbm_drift(ctx, c_devloc(f2), c_devloc(f1)).
+! Return values are 0 on success or a negative LBM_ERR_* code.
+!
+! Each per-call function replaces the reference subroutine named beside it,
+! with the arrays in the same order; dimensions and options come from the
+! lbm_params given to lbm_create (the reference reads them from the modules
+! mod_dimensions and m_readinfile).
+module lbm_b200_iface
+   use iso_c_binding
+   implicit none
+
+   integer(c_int), parameter :: LBM_OK = 0
+   integer(c_int), parameter :: LBM_ERR_ARG = -1, LBM_ERR_UNSUPPORTED = -2, LBM_ERR_CUDA = -3
+   integer(c_int), parameter :: LBM_ERR_STATE = -4, LBM_ERR_NUMERIC = -5, LBM_ERR_OOM = -6
+   integer(c_int32_t), parameter :: LBM_STORE_F32 = 0, LBM_STORE_F16 = 1
+
+   type, bind(C) :: lbm_params
+      integer(c_int32_t) :: nx, ny, nz, nl, ibgk, ihrr, ivreman, ibnd, jbnd, kbnd, iturb_pos, storage
+      real(c_float)      :: kinevisc, smagorinsky, rho0, udir
+   end type
+
+   interface
+      ! ---- context ------------------------------------------------------------------
+      integer(c_int) function lbm_create(ctx, p) bind(C, name="lbm_create")
+         import :: c_ptr, c_int, lbm_params
+         type(c_ptr), intent(out)     :: ctx
+         type(lbm_params), intent(in) :: p
+      end function
+      integer(c_int) function lbm_destroy(ctx) bind(C, name="lbm_destroy")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx
+      end function
+      type(c_ptr) function lbm_last_error(ctx) bind(C, name="lbm_last_error")
+         import :: c_ptr
+         type(c_ptr), value :: ctx
+      end function
+      integer(c_int) function lbm_set_stream(ctx, stream) bind(C, name="lbm_set_stream")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, stream
+      end function
+      integer(c_int) function lbm_synchronize(ctx) bind(C, name="lbm_synchronize")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx
+      end function
+
+      ! ---- per-call entry points (reference subroutines) ---------------------------------
+      ! call fequil3(feq,rho,u,v,w)                       m_fequil3.F90:4
+      integer(c_int) function lbm_fequil3(ctx, feq, rho, u, v, w) bind(C, name="lbm_fequil3")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, feq, rho, u, v, w
+      end function
+      ! call postcoll(f,tau,rho,u,v,w)                    m_postcoll.F90:4 (ablvisc may be c_null_ptr)
+      integer(c_int) function lbm_postcoll(ctx, f, tau, rho, u, v, w, ablvisc) bind(C, name="lbm_postcoll")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, tau, rho, u, v, w, ablvisc
+      end function
+      ! call drift(f,feq)                                 m_drift.F90:3
+      integer(c_int) function lbm_drift(ctx, f, feq) bind(C, name="lbm_drift")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      ! call macrovars(rho,u,v,w,f)                       m_macrovars.F90:4
+      integer(c_int) function lbm_macrovars(ctx, rho, u, v, w, f) bind(C, name="lbm_macrovars")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, rho, u, v, w, f
+      end function
+      ! call regularization(f,feq,u,v,w)                  m_regularization.F90:4
+      integer(c_int) function lbm_regularization(ctx, f, feq, u, v, w) bind(C, name="lbm_regularization")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq, u, v, w
+      end function
+      ! call vreman(f,tau)                                m_vreman.F90:187
+      integer(c_int) function lbm_vreman(ctx, f, tau) bind(C, name="lbm_vreman")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, tau
+      end function
+      ! call compute_fneq(f,feq)                          m_compute_fneq.F90:4
+      integer(c_int) function lbm_compute_fneq(ctx, f, feq) bind(C, name="lbm_compute_fneq")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      ! call compute_f(f,feq)                             m_compute_f.F90:84
+      integer(c_int) function lbm_compute_f(ctx, f, feq) bind(C, name="lbm_compute_f")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      ! call boundarycond(f1,f2,uvel,tracer,pottemp)      m_boundarycond.F90:14
+      integer(c_int) function lbm_boundarycond(ctx, f1, f2, uvel) bind(C, name="lbm_boundarycond")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f1, f2, uvel
+      end function
+      ! call solids(f,lblanking)                          m_solids.F90:3
+      integer(c_int) function lbm_solids(ctx, f, blanking) bind(C, name="lbm_solids")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, blanking
+      end function
+      ! call inflow_turbulence_forcing(rho,u,v,w,ampl,it,nrturb)   m_inflow_turbulence_forcing.F90:5
+      integer(c_int) function lbm_inflow_turbulence_forcing(ctx, df, rho, u, v, w, uu, vv, ww, ampl, it, nrturb) &
+            bind(C, name="lbm_inflow_turbulence_forcing")
+         import :: c_ptr, c_int, c_float, c_int32_t
+         type(c_ptr), value        :: ctx, df, rho, u, v, w, uu, vv, ww
+         real(c_float), value      :: ampl
+         integer(c_int32_t), value :: it, nrturb
+      end function
+      ! call inflow_turbulence_apply(f,turbulence_df)     m_inflow_turbulence_apply.F90:4
+      integer(c_int) function lbm_inflow_turbulence_apply(ctx, f, df) bind(C, name="lbm_inflow_turbulence_apply")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, df
+      end function
+      ! call fillghosts(f)                                m_fillghosts.F90:4
+      integer(c_int) function lbm_fillghosts(ctx, f) bind(C, name="lbm_fillghosts")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f
+      end function
+
+      ! ---- fused state API ----------------------------------------------------------------
+      integer(c_int) function lbm_state_import(ctx, f1, f2, rho, u, v, w, it) bind(C, name="lbm_state_import")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx, f1, f2, rho, u, v, w
+         integer(c_int32_t), value :: it
+      end function
+      integer(c_int) function lbm_state_export(ctx, f1, f2) bind(C, name="lbm_state_export")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f1, f2
+      end function
+      integer(c_int) function lbm_get_macro(ctx, rho, u, v, w) bind(C, name="lbm_get_macro")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, rho, u, v, w
+      end function
+      integer(c_int) function lbm_set_solids(ctx, blanking) bind(C, name="lbm_set_solids")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, blanking
+      end function
+      integer(c_int) function lbm_set_turbulence(ctx, uu, vv, ww, nrturb, ampl) bind(C, name="lbm_set_turbulence")
+         import :: c_ptr, c_int, c_float, c_int32_t
+         type(c_ptr), value        :: ctx, uu, vv, ww
+         integer(c_int32_t), value :: nrturb
+         real(c_float), value      :: ampl
+      end function
+      integer(c_int) function lbm_set_inflow(ctx, uvel) bind(C, name="lbm_set_inflow")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, uvel
+      end function
+      integer(c_int) function lbm_step(ctx, nsteps) bind(C, name="lbm_step")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx
+         integer(c_int32_t), value :: nsteps
+      end function
+      integer(c_int) function lbm_step_host(ctx, nsteps, uvel_host, status) bind(C, name="lbm_step_host")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx, uvel_host
+         integer(c_int32_t), value :: nsteps
+         integer(c_int32_t)        :: status
+      end function
+      integer(c_int) function lbm_status(ctx, flags) bind(C, name="lbm_status")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value :: ctx
+         integer(c_int32_t) :: flags
+      end function
+   end interface
+end module lbm_b200_iface

@@ -19,8 +19,10 @@ struct AosAcc {
     __device__ __forceinline__ float* p(int l, int i, int j, int k) const { return f + g.cell(i, j, k) * g.nl + l; }
     __device__ __forceinline__ float ld(int l, int i, int j, int k) const { return *p(l, i, j, k); }
     __device__ __forceinline__ void st(int l, int i, int j, int k, float v) const { *p(l, i, j, k) = v; }
-    __device__ __forceinline__ void cp(int l, int i, int j, int k, const AosAcc& s, int si, int sj, int sk) const {
-        *p(l, i, j, k) = *s.p(l, si, sj, sk);
+    // this(ld,i,j,k) = s(ls,si,sj,sk)
+    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const AosAcc& s, int ls, int si, int sj,
+                                       int sk) const {
+        *p(ld, i, j, k) = *s.p(ls, si, sj, sk);
     }
 };
 
@@ -32,8 +34,10 @@ struct SoaAcc {
     __device__ __forceinline__ S* p(int l, int i, int j, int k) const { return f + (long long)l * g.dstride + g.off(i, j, k); }
     __device__ __forceinline__ float ld(int l, int i, int j, int k) const { return Store<S>::to_f(*p(l, i, j, k)); }
     __device__ __forceinline__ void st(int l, int i, int j, int k, float v) const { *p(l, i, j, k) = Store<S>::from_f(v); }
-    __device__ __forceinline__ void cp(int l, int i, int j, int k, const SoaAcc& s, int si, int sj, int sk) const {
-        *p(l, i, j, k) = *s.p(l, si, sj, sk);
+    // this(ld,i,j,k) = s(ls,si,sj,sk), copied in storage type (exact)
+    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const SoaAcc& s, int ls, int si, int sj,
+                                       int sk) const {
+        *p(ld, i, j, k) = *s.p(ls, si, sj, sk);
     }
 };
 
@@ -57,16 +61,16 @@ __global__ void k_periodic(Acc a, int axis, int nl) {
     if (l >= nl) return;
     if (axis == 0) {            // (j,k) over (0..ny+1) x (0..nz+1); t = j, s = k
         if (t > ny + 1) return;
-        a.cp(l, 0, t, s, a, nx, t, s);
-        a.cp(l, nx + 1, t, s, a, 1, t, s);
+        a.cp(l, 0, t, s, a, l, nx, t, s);
+        a.cp(l, nx + 1, t, s, a, l, 1, t, s);
     } else if (axis == 1) {     // t = i, s = k
         if (t > nx + 1) return;
-        a.cp(l, t, 0, s, a, t, ny, s);
-        a.cp(l, t, ny + 1, s, a, t, 1, s);
+        a.cp(l, t, 0, s, a, l, t, ny, s);
+        a.cp(l, t, ny + 1, s, a, l, t, 1, s);
     } else {                    // t = i, s = j
         if (t > nx + 1) return;
-        a.cp(l, t, s, 0, a, t, s, nz);
-        a.cp(l, t, s, nz + 1, a, t, s, 1);
+        a.cp(l, t, s, 0, a, l, t, s, nz);
+        a.cp(l, t, s, nz + 1, a, l, t, s, 1);
     }
 }
 
@@ -95,11 +99,11 @@ __global__ void k_closed(Acc f1, Acc f2, int axis, FacePairs lo, FacePairs hi, i
     }
     for (int q = 0; q < fp.n; ++q) {
         const int l = fp.l[q], m = fp.m[q];
-        f1.cp(m, i, j, k, f2, i, j, k);
+        f1.cp(m, i, j, k, f2, l, i, j, k);
         const int si = (axis == 0) ? pi : pi - fp.cx[q];
         const int sj = (axis == 1) ? pj : pj - fp.cy[q];
         const int sk = (axis == 2) ? pk : pk - fp.cz[q];
-        f1.cp(l, i, j, k, f1, si, sj, sk);
+        f1.cp(l, i, j, k, f1, l, si, sj, sk);
     }
 }
 
@@ -123,8 +127,8 @@ __global__ void k_edges(Acc f1, Acc f2, EdgeSet es) {
     const EdgeDesc& d = es.e[blockIdx.y];
     const int i = d.gi < 0 ? t : d.gi, j = d.gj < 0 ? t : d.gj, k = d.gk < 0 ? t : d.gk;
     const int si = d.si < 0 ? t : d.si, sj = d.sj < 0 ? t : d.sj, sk = d.sk < 0 ? t : d.sk;
-    for (int q = 0; q < d.n; ++q) f1.cp(d.m[q], i, j, k, f2, i, j, k);
-    for (int q = 0; q < d.n; ++q) f1.cp(d.l[q], i, j, k, f1, si, sj, sk);
+    for (int q = 0; q < d.n; ++q) f1.cp(d.m[q], i, j, k, f2, d.l[q], i, j, k);
+    for (int q = 0; q < d.n; ++q) f1.cp(d.l[q], i, j, k, f1, d.l[q], si, sj, sk);
 }
 
 // The eight corners when all three axes are closed (m_boundary_closed_corners.F90).
@@ -138,8 +142,8 @@ __global__ void k_corners(Acc f1, Acc f2, CornerSet cs) {
     const int t = threadIdx.x;
     if (t >= 8 || cs.l[t] < 0) return;
     const int i = cs.ci[t], j = cs.cj[t], k = cs.ck[t];
-    f1.cp(cs.m[t], i, j, k, f2, i, j, k);
-    f1.cp(cs.l[t], i, j, k, f1, i - cs.cx[t], j - cs.cy[t], k - cs.cz[t]);
+    f1.cp(cs.m[t], i, j, k, f2, cs.l[t], i, j, k);
+    f1.cp(cs.l[t], i, j, k, f1, cs.l[t], i - cs.cx[t], j - cs.cy[t], k - cs.cz[t]);
 }
 
 // Inflow at i=0 and zero-gradient outflow at i=nx+1, m_boundary_i_inflow_kernel.F90:161-231.
@@ -167,7 +171,7 @@ __global__ void k_inflow(Acc f, const float* __restrict__ uvel, float rho0, floa
         f.st(l, 0, j, k, v);
     }
 #pragma unroll
-    for (int l = 0; l < Q; ++l) f.cp(l, nx + 1, j, k, f, nx, j, k);
+    for (int l = 0; l < Q; ++l) f.cp(l, nx + 1, j, k, f, l, nx, j, k);
 }
 
 }  // namespace lbm

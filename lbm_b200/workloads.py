@@ -49,8 +49,11 @@ class Workload:
 SPHERE_128 = Workload("sphere_q27_128x64x64", 128, 64, 64, 27, steps=200, sphere=(32, 32, 32, 8))
 CHANNEL_Q27 = Workload("turb_inflow_q27_512x256x256", 512, 256, 256, 27, steps=1000, lturb=True, ampl=1.0e-4)
 CHANNEL_Q19 = CHANNEL_Q27.with_(name="turb_inflow_q19_512x256x256", nl=19)
+# one eighth of the channel, for profiler captures that must stay small
+CHANNEL_Q27_SMALL = CHANNEL_Q27.with_(name="turb_inflow_q27_256x128x128", nx=256, ny=128, nz=128)
+CHANNEL_Q19_SMALL = CHANNEL_Q27_SMALL.with_(name="turb_inflow_q19_256x128x128", nl=19)
 
-WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19)}
+WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL)}
 
 
 def initial_macro(wl: Workload, dtype=np.float32):
