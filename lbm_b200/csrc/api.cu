@@ -40,6 +40,9 @@ struct lbm_ctx {
     float* d_turb = nullptr;      // uu,vv,ww copies
     int nrturb = 0;
     float ampl = 0.f;
+    bool fold = false;            // boundaries folded into the step kernel (see state_kernels.cuh)
+    void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
+    int kopt_lo = 0, kopt_hi = 0;
     float* d_uvel = nullptr;      // uvel(nz)
     float* d_abl = nullptr;       // ablvisc(nz), zero unless set
     int* d_it = nullptr;          // number of the step being computed
@@ -242,6 +245,12 @@ void setup_boundaries(lbm_ctx* c) {
                         }
                 }
     }
+    // the reference's configuration (inflow/outflow i, periodic j, closed k) runs with folded boundaries
+    int ko1, koN;
+    closed_opts(kb, ko1, koN);
+    c->fold = (ib == 1 && jb == 0 && ko1 != 0);
+    c->kopt_lo = ko1;
+    c->kopt_hi = koN;
     // m_boundary_i_inflow_kernel.F90:191-193: cos(udir*pi/180), sin(udir*pi/180) in single precision
     const float pi = 3.1415927410125732f;
     c->cosd = cosf(c->p.udir * pi / 180.0f);
@@ -328,6 +337,15 @@ StepArgs step_args(lbm_ctx* c) {
     a.u_in = c->d_macro + g;
     a.v_in = c->d_macro + 2 * g;
     a.w_in = c->d_macro + 3 * g;
+    a.kopt_lo = c->kopt_lo;
+    a.kopt_hi = c->kopt_hi;
+    a.uvel = c->d_uvel;
+    a.rho0 = c->p.rho0;
+    a.cosd = c->cosd;
+    a.sind = c->sind;
+    a.d_it_rw = c->d_it;
+    a.edge = c->d_edge;
+    a.full_sector = (c->p.nx % (32 / (int)c->elem)) == 0;
     return a;
 }
 
@@ -338,14 +356,30 @@ int step_one(lbm_ctx* c) {
     StepArgs a = step_args(c);
     if (c->state == ST_PRE) {
         S* b = (S*)c->buf[c->cur];
-        k_step<Q, S, false><<<grd, 128, 0, c->stream>>>(b, b, a);
+        k_step<Q, S, false, false><<<grd, 128, 0, c->stream>>>(b, b, a);
         c->launches++;
         LBM_LAUNCHED(c, "collide");
         c->state = ST_POST;
+    } else if (c->fold) {
+        const int nxt = 1 - c->cur;
+        LBM_TRY(prof_begin(c));
+        k_step<Q, S, true, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        c->launches++;
+        LBM_LAUNCHED(c, "fused step");
+        LBM_TRY(prof_end(c));
+        const int nface = 2 * g.ny * ((g.nx + 127) / 128);
+        const long long nxg = (long long)Q * g.ny * g.nz;
+        const int nblk = nface + (int)((nxg + 127) / 128);
+        k_bc_fold<Q, S><<<nblk, 128, 0, c->stream>>>((S*)c->buf[nxt], (const S*)c->buf[c->cur], a, nface);
+        c->launches++;
+        LBM_LAUNCHED(c, "folded boundaries");
+        c->cur = nxt;
+        c->it += 1;
+        return LBM_OK;
     } else {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        k_step<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        k_step<Q, S, true, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
         c->launches++;
         LBM_LAUNCHED(c, "fused step");
         LBM_TRY(prof_end(c));
@@ -371,21 +405,25 @@ void launch_import(lbm_ctx* c, const float* ref, int b) {
     k_import<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(ref, (S*)c->buf[b], g);
     c->launches++;
 }
+// after a step, periodic-j ghost rows are read as rows ny and 1 (state_kernels.cuh)
+int wrap_rows(const lbm_ctx* c) { return (c->state == ST_POST && c->p.jbnd == 0) ? 1 : 0; }
+
 template <int Q, typename S>
 void launch_export(lbm_ctx* c, float* ref, int b, bool pull) {
     const SoaGrid& g = c->sg;
     dim3 grd((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2);
     if (pull)
-        k_export<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], (const S*)c->buf[1 - b], ref, g);
+        k_export<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], (const S*)c->buf[1 - b], ref, g,
+                                                        wrap_rows(c));
     else
-        k_export<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], nullptr, ref, g);
+        k_export<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], nullptr, ref, g, wrap_rows(c));
     c->launches++;
 }
 template <int Q, typename S>
 void launch_macro(lbm_ctx* c, float* rho, float* u, float* v, float* w) {
     const SoaGrid& g = c->sg;
     k_macro<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(
-        (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g);
+        (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g, wrap_rows(c));
     c->launches++;
 }
 
@@ -445,6 +483,7 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     const size_t g = (size_t)c->rg.ncell();
     chk(cudaMalloc(&c->d_macro, 4 * g * sizeof(float)), "cudaMalloc(macro)");
     chk(cudaMalloc(&c->d_uvel, (size_t)p->nz * sizeof(float)), "cudaMalloc(uvel)");
+    chk(cudaMalloc(&c->d_edge, (size_t)2 * p->nl * p->ny * p->nz * c->elem), "cudaMalloc(edge)");
     chk(cudaMalloc(&c->d_abl, (size_t)p->nz * sizeof(float)), "cudaMalloc(ablvisc)");
     chk(cudaMalloc(&c->d_it, 2 * sizeof(int)), "cudaMalloc(step)");
     chk(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc(status)");
@@ -472,6 +511,7 @@ int lbm_destroy(lbm_ctx* c) {
     cudaFree(c->d_solid);
     cudaFree(c->d_turb);
     cudaFree(c->d_uvel);
+    cudaFree(c->d_edge);
     cudaFree(c->d_abl);
     cudaFree(c->d_it);
     cudaFree(c->d_status);

@@ -39,6 +39,28 @@ __host__ __device__ constexpr float lat_w(int l) {
                                            : 1.0f / 216.0f);
 }
 __host__ __device__ constexpr int lat_opposite(int l) { return l == 0 ? 0 : ((l & 1) ? l + 1 : l - 1); }
+// index of direction (x,y,z) among the first Q directions, -1 if absent
+template <int Q>
+__host__ __device__ constexpr int lat_find(int x, int y, int z) {
+    for (int m = 0; m < Q; ++m)
+        if (lat_cx(m) == x && lat_cy(m) == y && lat_cz(m) == z) return m;
+    return -1;
+}
+
+// The same tables in constant memory, for kernels that index directions at run time.
+#define LBM_27(F) F(0), F(1), F(2), F(3), F(4), F(5), F(6), F(7), F(8), F(9), F(10), F(11), F(12), F(13), \
+    F(14), F(15), F(16), F(17), F(18), F(19), F(20), F(21), F(22), F(23), F(24), F(25), F(26)
+#define LBM_CX(l) lat_cx(l)
+#define LBM_CY(l) lat_cy(l)
+#define LBM_CZ(l) lat_cz(l)
+#define LBM_OPP(l) lat_opposite(l)
+#define LBM_W19(l) lat_w<19>(l)
+#define LBM_W27(l) lat_w<27>(l)
+__constant__ int8_t c_cx[27] = {LBM_27(LBM_CX)};
+__constant__ int8_t c_cy[27] = {LBM_27(LBM_CY)};
+__constant__ int8_t c_cz[27] = {LBM_27(LBM_CZ)};
+__constant__ int8_t c_opp[27] = {LBM_27(LBM_OPP)};
+__constant__ float c_w[2][27] = {{LBM_27(LBM_W19)}, {LBM_27(LBM_W27)}};   // [0] D3Q19, [1] D3Q27
 
 // ---------------------------------------------------------------------------
 // Reference layout f(nl,0:nx+1,0:ny+1,0:nz+1), l fastest (Fortran column-major).
@@ -55,8 +77,10 @@ struct RefGrid {
 // Structure-of-arrays layout of the fused state.  Each direction is a block of
 // (ny+2)*(nz+2) rows of `pitch` elements; in a row, ghost i=0 sits at offset
 // 31 so that the interior i=1..nx starts on a 128-byte boundary (FP32) and a
-// warp of consecutive i writes whole cache lines.  pitch = roundup(nx+2, 32)
-// leaves room for ghost nx+1 before the next row's ghost 0.
+// warp of consecutive i writes whole cache lines.  pitch = roundup(nx+34, 32)
+// leaves at least 34 elements of padding per row, so that (for nx a multiple
+// of the sector's element count) the 32-byte sectors holding ghost i=0 and
+// ghost nx+1 contain nothing else: the boundary kernel writes them whole.
 // ---------------------------------------------------------------------------
 struct SoaGrid {
     int nx, ny, nz;
@@ -71,7 +95,7 @@ struct SoaGrid {
     static SoaGrid make(int nx, int ny, int nz) {
         SoaGrid g;
         g.nx = nx; g.ny = ny; g.nz = nz;
-        g.pitch = ((nx + 2 + 31) / 32) * 32;
+        g.pitch = ((nx + 34 + 31) / 32) * 32;
         g.rowsz = g.pitch;
         g.dstride = (long long)(ny + 2) * (nz + 2) * g.pitch + 32;
         return g;

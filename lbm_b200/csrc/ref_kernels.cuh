@@ -12,9 +12,6 @@
 
 namespace lbm {
 
-__constant__ int8_t c_cx[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1};
-__constant__ int8_t c_cy[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 0, 0, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
-__constant__ int8_t c_cz[27] = {0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1};
 
 // Equilibrium offsets feq_l - w_l (m_fequil3_kernel.F90:112-167 in closed form).
 template <int Q>

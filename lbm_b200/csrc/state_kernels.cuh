@@ -5,9 +5,21 @@
 // inflow_turbulence_apply -> solids (main.F90:322-329 of step n-1 and
 // :296-310 of step n): it pulls the post-collision populations of the
 // neighbours, forms the moments in registers, collides, and writes the new
-// post-collision populations once.  The boundary ghost kernels then run in the
-// reference's order on the new buffer, reading the old buffer's ghosts for
-// the two-step bounce-back.
+// post-collision populations once.
+//
+// Boundaries.  In the general case the ghost kernels of boundary.cuh then run
+// in the reference's order.  For the configuration the reference runs
+// (inflow/outflow in i, periodic j, closed k: ibnd=1, jbnd=0, kbnd in
+// {11,12,21,22}) the step kernel also writes the ghost cells itself ("folded"
+// boundaries), reproducing boundarycond (m_boundarycond.F90:108-365) value
+// for value, with one extra launch instead of four:
+//   * periodic j: the ghost rows j=0 and ny+1 are never stored; every reader
+//     wraps the row index instead.  After boundarycond the reference's ghost
+//     rows are exact copies of rows ny and 1, so wrapping reads the same data.
+//   * closed k and inflow/outflow in one kernel, k_bc_fold, in which the
+//     reference's ordering (k-faces read x-ghost columns before the inflow
+//     rewrites them) is kept by giving each x-ghost element a single thread
+//     that reads its old value and then writes the new one.
 #pragma once
 
 #include "collide.cuh"
@@ -32,6 +44,13 @@ struct StepArgs {
     const float* u_in;
     const float* v_in;
     const float* w_in;
+    // folded boundaries
+    int kopt_lo, kopt_hi;     // -1 no-slip, +1 free-slip at k=1 / k=nz
+    const float* uvel;        // inflow profile uvel(nz)
+    float rho0, cosd, sind;   // inflow constants (m_boundary_i_inflow_kernel.F90:191-193)
+    int* d_it_rw;             // step counter, advanced by the boundary kernel
+    void* edge;               // post-collision populations at i=1 and i=nx: [side][l][k-1][j-1]
+    int full_sector;          // x-ghost sectors hold nothing but the ghost and padding
 };
 
 __device__ __forceinline__ void flag_bad_density(int* status, float rho, float ux, float uy, float uz) {
@@ -58,25 +77,153 @@ __device__ __forceinline__ TurbIn turb_at(const StepArgs& a, int i, int j, int k
     return tb;
 }
 
+// periodic row index for j in 0..ny+1
+__device__ __forceinline__ int wrapj(int j, int ny) { return j == 0 ? ny : (j == ny + 1 ? 1 : j); }
+
+// element distance from cell (i,j,k) back to its pull source (i-cx, j-cy, k-cz);
+// with wrap, a source row 0 or ny+1 is replaced by row ny or 1 (j interior)
+template <int L>
+__device__ __forceinline__ long long pull_delta(const SoaGrid& g, int j, bool wrap) {
+    const long long rs = g.pitch, ps = (long long)g.pitch * (g.ny + 2);
+    long long d = lat_cx(L) + lat_cy(L) * rs + lat_cz(L) * ps;
+    if (wrap) {
+        if (lat_cy(L) > 0 && j == 1) d -= (long long)g.ny * rs;
+        if (lat_cy(L) < 0 && j == g.ny) d += (long long)g.ny * rs;
+    }
+    return d;
+}
+
+template <int Q, typename S, int L>
+struct PullLoop {
+    static __device__ __forceinline__ void run(float (&fp)[Q], const S* src, const SoaGrid& g, long long o, int j,
+                                               bool wrap) {
+        fp[L] = Store<S>::load(src + (long long)L * g.dstride + o - pull_delta<L>(g, j, wrap));
+        PullLoop<Q, S, L + 1>::run(fp, src, g, o, j, wrap);
+    }
+};
+template <int Q, typename S>
+struct PullLoop<Q, S, Q> {
+    static __device__ __forceinline__ void run(float (&)[Q], const S*, const SoaGrid&, long long, int, bool) {}
+};
+
+// Store one 32-byte sector (two 16-byte vectors) holding v at element `slot`
+// and zeros elsewhere; p is 32-byte aligned.
+template <typename S>
+__device__ __forceinline__ void store_sector(S* p, S v, int slot) {
+    unsigned int w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+    if (sizeof(S) == 4) {
+        w[slot] = *reinterpret_cast<const unsigned int*>(&v);
+    } else {
+        const unsigned int h = *reinterpret_cast<const unsigned short*>(&v);
+        w[slot >> 1] = (slot & 1) ? (h << 16) : h;
+    }
+    uint4* q = reinterpret_cast<uint4*>(p);
+    q[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    q[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// Boundary kernel of the folded configuration, run after k_step on the new
+// buffer f1 (= dst of the step) with f2 the old buffer.  Two kinds of threads:
+//   * k-face threads, one per (i, j, face) with i in 1..nx: for each outgoing
+//     direction l of the face, f1(l,i,j,kg) = f1(l, i-cx, j-cy, kp) when the
+//     source is an interior cell, and f1(m,i,j,kg) = f2(l,i,j,kg) for the
+//     reflected direction m (m_boundary_k_closed_kernel.F90:157-168).
+//   * x-ghost threads, one per (l, j, k): the inflow value of ghost (0,j,k)
+//     and the outflow value of ghost (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:
+//     184-231).  At the planes k=1 and k=nz they first pass the value their
+//     x-ghost held before this step to the k-ghost cell that the reference's
+//     k-face copies it to (sources i-cx = 0 or nx+1), so each x-ghost element is
+//     read and then written by one and the same thread.
+template <int Q, typename S>
+__global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
+    const SoaGrid& g = a.g;
+    if ((int)blockIdx.x < nface_blocks) {
+        const int per_row = (g.nx + 127) / 128;
+        const int b = blockIdx.x;
+        const int side = b / (per_row * g.ny);
+        const int j = (b / per_row) % g.ny + 1;
+        const int i = (b % per_row) * 128 + threadIdx.x + 1;
+        if (i > g.nx) return;
+        const int kp = side ? g.nz : 1, kg = side ? g.nz + 1 : 0;
+        const int opt = side ? a.kopt_hi : a.kopt_lo;
+#pragma unroll
+        for (int l = 1; l < Q; ++l) {
+            const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+            const bool out = side ? (cz > 0) : (cz < 0);
+            if (!out) continue;
+            const int si = i - cx;
+            if (si >= 1 && si <= g.nx)
+                f1[(long long)l * g.dstride + g.off(i, j, kg)] = f1[(long long)l * g.dstride + g.off(si, wrapj(j - cy, g.ny), kp)];
+            const int m = opt < 0 ? lat_opposite(l) : lat_find<Q>(cx, cy, -cz);
+            f1[(long long)m * g.dstride + g.off(i, j, kg)] = f2[(long long)l * g.dstride + g.off(i, j, kg)];
+        }
+        return;
+    }
+    // x-ghost threads
+    const long long e = (long long)(blockIdx.x - nface_blocks) * blockDim.x + threadIdx.x;
+    const long long nyz = (long long)g.ny * g.nz;
+    if (e >= (long long)Q * nyz) return;
+    if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
+    const int j = (int)(e % g.ny) + 1;
+    const int l = (int)((e / g.ny) % Q);
+    const int k = (int)(e / ((long long)g.ny * Q)) + 1;
+    const int cx = c_cx[l], cy = c_cy[l], cz = c_cz[l];
+    S* fl = f1 + (long long)l * g.dstride;
+    if (k == 1 || k == g.nz) {
+        // stale x-ghost values feed the k-face ghost cells (1,.,kg) and (nx,.,kg)
+        const bool out = (k == 1) ? (cz < 0) : (cz > 0);
+        if (out) {
+            const int kg = (k == 1) ? 0 : g.nz + 1;
+            if (cx > 0) fl[g.off(1, wrapj(j + cy, g.ny), kg)] = fl[g.off(0, j, k)];
+            if (cx < 0) fl[g.off(g.nx, wrapj(j + cy, g.ny), kg)] = fl[g.off(g.nx + 1, j, k)];
+        }
+    }
+    const S* edge = (const S*)a.edge;
+    const long long cell = (long long)(k - 1) * g.ny + (j - 1);
+    // inflow: directions with cx > 0 take the corrected value of their opposite
+    const int ls = (cx > 0) ? c_opp[l] : l;
+    const float wl = c_w[Q == 27 ? 1 : 0][ls];
+    const float cxl = (float)c_cx[ls], cyl = (float)c_cy[ls];
+    const float uu = a.uvel[k - 1];
+    const float cs2 = 1.0f / 3.0f;
+    const float fin = Store<S>::to_f(edge[(long long)ls * nyz + cell]);
+    const S gin = Store<S>::from_f(fin - 2.0f * wl * a.rho0 * (cxl * uu * a.cosd + cyl * uu * a.sind) / cs2);
+    // outflow: zero gradient
+    const S gout = edge[((long long)Q + l) * nyz + cell];
+    S* pin = fl + g.off(0, j, k);
+    S* pout = fl + g.off(g.nx + 1, j, k);
+    if (a.full_sector) {
+        // write each ghost's whole 32-byte sector (the rest is row padding) so the
+        // store needs no read-modify-write of a partial sector
+        constexpr int spe = 32 / (int)sizeof(S);
+        store_sector<S>(pin - (spe - 1), gin, spe - 1);
+        store_sector<S>(pout, gout, 0);
+    } else {
+        *pin = gin;
+        *pout = gout;
+    }
+}
+
 // PULL = true : dst(interior) = collide(pull(src))        (steady fused step)
 // PULL = false: dst == src, collide in place with rho,u from the arrays in a
 //               (the first step after an import, whose moments the caller gave)
-template <int Q, typename S, bool PULL>
-__global__ void __launch_bounds__(128) k_step(const S* src, S* dst, StepArgs a) {
+// WRAP = true : folded configuration: periodic j without stored ghost rows, and
+//               the populations at i=1 and i=nx copied to the edge array
+template <int Q, typename S, bool PULL, bool WRAP>
+__global__ void __launch_bounds__(128, 8) k_step(const S* src, S* dst, StepArgs a) {
     const SoaGrid g = a.g;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y + 1;
     const int k = blockIdx.z + 1;
     if (i > g.nx) return;
     const long long o = g.off(i, j, k);
-    const long long rs = g.pitch;
-    const long long ps = (long long)g.pitch * (g.ny + 2);
 
     float fp[Q];
+    if (PULL) {
+        PullLoop<Q, S, 0>::run(fp, src, g, o, j, WRAP);
+    } else {
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        const long long d = PULL ? (lat_cx(l) + lat_cy(l) * rs + lat_cz(l) * ps) : 0;
-        fp[l] = Store<S>::load(src + (long long)l * g.dstride + o - d);
+        for (int l = 0; l < Q; ++l) fp[l] = Store<S>::load(src + (long long)l * g.dstride + o);
     }
     const Moments m = moments<Q>(fp);
     float rho, drho, ux, uy, uz;
@@ -102,6 +249,13 @@ __global__ void __launch_bounds__(128) k_step(const S* src, S* dst, StepArgs a) 
     collide<Q>(fp, m, drho, rho, ux, uy, uz, a.cp, abl, a.cp.tau0, solid, tb);
 #pragma unroll
     for (int l = 0; l < Q; ++l) Store<S>::store(dst + (long long)l * g.dstride + o, fp[l]);
+    if (WRAP && (i == 1 || i == g.nx)) {
+        // the boundary kernel builds the inflow/outflow ghosts from these, read coalesced
+        const long long nyz = (long long)g.ny * g.nz;
+        S* e = (S*)a.edge + (i == 1 ? 0 : (long long)Q * nyz) + (long long)(k - 1) * g.ny + (j - 1);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) e[l * nyz] = Store<S>::from_f(fp[l]);
+    }
 }
 
 // Advance the device step counter after the boundary kernels of a step.
@@ -130,12 +284,26 @@ __global__ void __launch_bounds__(128) k_import(const float* __restrict__ ref, S
     }
 }
 
+template <int Q, typename S, int L>
+struct PullMacro {
+    static __device__ __forceinline__ void run(float (&fp)[Q], const S* src, const SoaGrid& g, long long o, int j,
+                                               bool wrap) {
+        fp[L] = Store<S>::to_f(src[(long long)L * g.dstride + o - pull_delta<L>(g, j, wrap)]);
+        PullMacro<Q, S, L + 1>::run(fp, src, g, o, j, wrap);
+    }
+};
+template <int Q, typename S>
+struct PullMacro<Q, S, Q> {
+    static __device__ __forceinline__ void run(float (&)[Q], const S*, const SoaGrid&, long long, int, bool) {}
+};
+
 // State -> reference layout.  PULL: interior cells take the streamed values
 // pulled from `src` (the reference's f1 after drift), ghost cells are copied
-// from `ghost`.  Otherwise every cell is copied from `src`.
+// from `ghost`.  Otherwise every cell is copied from `src`.  wrap: periodic j,
+// ghost rows read from rows ny and 1 (see the file header).
 template <int Q, typename S, bool PULL>
 __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const S* __restrict__ ghost,
-                                                float* __restrict__ ref, SoaGrid g) {
+                                                float* __restrict__ ref, SoaGrid g, int wrap) {
     __shared__ float sm[128 * Q];
     const int i0 = blockIdx.x * 128;
     const int j = blockIdx.y, k = blockIdx.z;
@@ -145,19 +313,17 @@ __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const
     if (t < n) {
         const int i = i0 + t;
         const bool interior = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
-        const long long o = g.off(i, j, k);
-        const long long rs = g.pitch, ps = (long long)g.pitch * (g.ny + 2);
+        float v[Q];
+        if (PULL && interior) {
+            PullMacro<Q, S, 0>::run(v, src, g, g.off(i, j, k), j, wrap != 0);
+        } else {
+            const long long o = g.off(i, wrap ? wrapj(j, g.ny) : j, k);
+            const S* s = PULL ? ghost : src;
 #pragma unroll
-        for (int l = 0; l < Q; ++l) {
-            float v;
-            if (PULL && interior) {
-                const long long d = lat_cx(l) + lat_cy(l) * rs + lat_cz(l) * ps;
-                v = Store<S>::to_f(src[(long long)l * g.dstride + o - d]);
-            } else {
-                v = Store<S>::to_f((PULL ? ghost : src)[(long long)l * g.dstride + o]);
-            }
-            sm[t * Q + l] = v + lat_w<Q>(l);
+            for (int l = 0; l < Q; ++l) v[l] = Store<S>::to_f(s[(long long)l * g.dstride + o]);
         }
+#pragma unroll
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = v[l] + lat_w<Q>(l);
     }
     __syncthreads();
     const long long base = ((long long)i0 + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k)) * Q;
@@ -168,18 +334,18 @@ __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const
 // from the pulled values of `src`, ghost cells from `ghost` itself.
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_macro(const S* __restrict__ src, const S* __restrict__ ghost, float* rho,
-                                               float* u, float* v, float* w, SoaGrid g) {
+                                               float* u, float* v, float* w, SoaGrid g, int wrap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i > g.nx + 1) return;
     const bool interior = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
-    const long long o = g.off(i, j, k);
-    const long long rs = g.pitch, ps = (long long)g.pitch * (g.ny + 2);
     float fp[Q];
+    if (interior) {
+        PullMacro<Q, S, 0>::run(fp, src, g, g.off(i, j, k), j, wrap != 0);
+    } else {
+        const long long o = g.off(i, wrap ? wrapj(j, g.ny) : j, k);
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        const long long d = interior ? (lat_cx(l) + lat_cy(l) * rs + lat_cz(l) * ps) : 0;
-        fp[l] = Store<S>::to_f((interior ? src : ghost)[(long long)l * g.dstride + o - d]);
+        for (int l = 0; l < Q; ++l) fp[l] = Store<S>::to_f(ghost[(long long)l * g.dstride + o]);
     }
     const Moments m = moments<Q>(fp);
     const float r = 1.0f + m.s0;
