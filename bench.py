@@ -336,7 +336,7 @@ def main():
     bl = bytes_per_lup(wl.nl, a.storage)
     k_ms = kms / max(kn, 1)
     achieved = cells * bl / (k_ms * 1e-3) / 1e9 if kn else None
-    key = "k_step<%d,%s,true>" % (wl.nl, "float" if a.storage == "f32" else "__half")
+    key = "k_step_fast<%d,%s>" % (wl.nl, "float" if a.storage == "f32" else "__half")
     traffic = ncu_traffic(key, cells)
     line = {"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",

@@ -42,6 +42,7 @@ struct lbm_ctx {
     float ampl = 0.f;
     bool fold = false;            // boundaries folded into the step kernel (see state_kernels.cuh)
     void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
+    bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
     int kopt_lo = 0, kopt_hi = 0;
     float* d_uvel = nullptr;      // uvel(nz)
     float* d_abl = nullptr;       // ablvisc(nz), zero unless set
@@ -346,6 +347,15 @@ StepArgs step_args(lbm_ctx* c) {
     a.d_it_rw = c->d_it;
     a.edge = c->d_edge;
     a.full_sector = (c->p.nx % (32 / (int)c->elem)) == 0;
+    {
+        const SoaGrid& g = c->sg;
+        const long long plane = (long long)g.pitch * (g.ny + 2);
+        for (int l = 0; l < c->p.nl; ++l) {
+            const long long d = lat_cx(l) + (long long)lat_cy(l) * g.pitch + (long long)lat_cz(l) * plane;
+            a.poff[l] = (int)((long long)l * g.dstride - d);
+            a.soff[l] = (int)((long long)l * g.dstride);
+        }
+    }
     return a;
 }
 
@@ -363,7 +373,10 @@ int step_one(lbm_ctx* c) {
     } else if (c->fold) {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        k_step<Q, S, true, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        if (c->idx32)
+            k_step_fast<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        else
+            k_step<Q, S, true, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
         c->launches++;
         LBM_LAUNCHED(c, "fused step");
         LBM_TRY(prof_end(c));
@@ -379,7 +392,10 @@ int step_one(lbm_ctx* c) {
     } else {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        k_step<Q, S, true, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        if (c->idx32)
+            k_step_fast<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+        else
+            k_step<Q, S, true, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
         c->launches++;
         LBM_LAUNCHED(c, "fused step");
         LBM_TRY(prof_end(c));
@@ -468,6 +484,7 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     c->cp.ihrr = p->ihrr;
     c->cp.ivreman = p->ivreman;
     c->elem = (p->storage == LBM_STORE_F16) ? 2 : 4;
+    c->idx32 = (long long)p->nl * c->sg.dstride < (1LL << 31);
     setup_boundaries(c);
     int rc = LBM_OK;
     auto chk = [&](cudaError_t e, const char* w) {

@@ -22,7 +22,7 @@
 //     that reads its old value and then writes the new one.
 #pragma once
 
-#include "collide.cuh"
+#include "collide_rows.cuh"
 
 namespace lbm {
 
@@ -51,6 +51,9 @@ struct StepArgs {
     int* d_it_rw;             // step counter, advanced by the boundary kernel
     void* edge;               // post-collision populations at i=1 and i=nx: [side][l][k-1][j-1]
     int full_sector;          // x-ghost sectors hold nothing but the ghost and padding
+    // 32-bit element offsets of k_step_fast, computed on the host:
+    int poff[27];             // pull source of direction l relative to the cell: l*dstride - (cx + cy*pitch + cz*plane)
+    int soff[27];             // l*dstride
 };
 
 __device__ __forceinline__ void flag_bad_density(int* status, float rho, float ux, float uy, float uz) {
@@ -255,6 +258,89 @@ __global__ void __launch_bounds__(128, 8) k_step(const S* src, S* dst, StepArgs 
         S* e = (S*)a.edge + (i == 1 ? 0 : (long long)Q * nyz) + (long long)(k - 1) * g.ny + (j - 1);
 #pragma unroll
         for (int l = 0; l < Q; ++l) e[l * nyz] = Store<S>::from_f(fp[l]);
+    }
+}
+
+// Pull loads of k_step_fast: direction L reads base + poff[L]; sources in row
+// j-1 (cy = +1) and j+1 (cy = -1) use bases shifted to the wrapped row.
+template <int Q, typename S, int L>
+struct Load32 {
+    static __device__ __forceinline__ void run(float (&fp)[Q], const S* p0, const S* pyp, const S* pym,
+                                               const StepArgs& a) {
+        const S* b = lat_cy(L) > 0 ? pyp : (lat_cy(L) < 0 ? pym : p0);
+        if constexpr (sizeof(S) == 2) fp[L] = __half2float(__ldg(b + a.poff[L]));   // 2^8-scaled
+        else fp[L] = __ldg(b + a.poff[L]);
+        Load32<Q, S, L + 1>::run(fp, p0, pyp, pym, a);
+    }
+};
+template <int Q, typename S>
+struct Load32<Q, S, Q> {
+    static __device__ __forceinline__ void run(float (&)[Q], const S*, const S*, const S*, const StepArgs&) {}
+};
+
+// Steady fused step with the row-organised collision (collide_rows.cuh).  FP16
+// state is used in its 2^8-scaled form: the moments are rescaled once and the
+// emission constants carry the scale, so no population is multiplied on the way
+// in or out.  Needs Q * dstride < 2^31 (32-bit element offsets).
+template <int Q, typename S, bool WRAP>
+__global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src, S* __restrict__ dst, StepArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > a.g.nx) return;
+    const long long o = a.g.off(i, j, k);
+    float fp[Q];
+    {
+        const S* p0 = src + o;
+        const long long wrapd = (long long)a.g.ny * a.g.pitch;
+        const S* pyp = (WRAP && j == 1) ? p0 + wrapd : p0;         // row 0 -> row ny
+        const S* pym = (WRAP && j == a.g.ny) ? p0 - wrapd : p0;    // row ny+1 -> row 1
+        Load32<Q, S, 0>::run(fp, p0, pyp, pym, a);
+    }
+    Moments m = moments_rows<Q>(fp);
+    constexpr float inv_scale = 1.0f / store_scale<S>();
+    if constexpr (sizeof(S) == 2) {
+        m.s0 *= inv_scale; m.jx *= inv_scale; m.jy *= inv_scale; m.jz *= inv_scale;
+        m.pxx *= inv_scale; m.pyy *= inv_scale; m.pzz *= inv_scale;
+        m.pxy *= inv_scale; m.pxz *= inv_scale; m.pyz *= inv_scale;
+    }
+    const float drho = m.s0;
+    const float rho = 1.0f + m.s0;
+    const float inv = __frcp_rn(rho);
+    const float ux = m.jx * inv, uy = m.jy * inv, uz = m.jz * inv;
+    flag_bad_density(a.status, rho, ux, uy, uz);
+    const bool solid = a.solid ? a.solid[((long long)(k - 1) * a.g.ny + (j - 1)) * a.g.nx + (i - 1)] != 0 : false;
+    const float abl = a.abl ? a.abl[k - 1] : 0.0f;
+    if (a.cp.ihrr) {
+        collide_rows<Q, S>(fp, m, drho, rho, ux, uy, uz, a.cp, abl, solid);
+        if (a.uu != nullptr && i == a.iturb) {
+            const TurbIn tb = turb_at(a, i, j, k);
+            add_turbulence<Q>(fp, rho, ux, uy, uz, tb, a.cp.ibgk == 3, solid, store_scale<S>());
+        }
+    } else {
+        // plain BGK on the unregularized non-equilibrium (collide.cuh)
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fp[l] *= inv_scale;
+        const TurbIn tb = turb_at(a, i, j, k);
+        collide<Q>(fp, m, drho, rho, ux, uy, uz, a.cp, abl, a.cp.tau0, solid, tb);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fp[l] *= store_scale<S>();
+    }
+    S* q = dst + o;
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        if constexpr (sizeof(S) == 2) q[a.soff[l]] = __float2half_rn(fp[l]);
+        else q[a.soff[l]] = fp[l];
+    }
+    if (WRAP && (i == 1 || i == a.g.nx)) {
+        // the boundary kernel builds the inflow/outflow ghosts from these, read coalesced
+        const long long nyz = (long long)a.g.ny * a.g.nz;
+        S* e = (S*)a.edge + (i == 1 ? 0 : (long long)Q * nyz) + (long long)(k - 1) * a.g.ny + (j - 1);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            if constexpr (sizeof(S) == 2) e[l * nyz] = __float2half_rn(fp[l]);
+            else e[l * nyz] = fp[l];
+        }
     }
 }
 
