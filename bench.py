@@ -14,7 +14,6 @@ exchange step between replicas); rank 0 prints one JSON line.
 from __future__ import annotations
 
 import argparse
-import datetime
 import json
 import os
 import statistics
@@ -258,6 +257,7 @@ def make_solver(wl, storage, seed):
 def timed_steps(s, steps, dist, profile=True):
     """Time exactly `steps` fused steps with CUDA events on the library's stream; max over ranks."""
     import torch
+    from lbm_b200 import replicas
     L = s.lbm
     if dist is not None:
         dist.barrier()
@@ -275,9 +275,7 @@ def timed_steps(s, steps, dist, profile=True):
     kms, kn = L.profile_read() if profile else (0.0, 0)
     L.profile(False)
     if dist is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = replicas.max_over_ranks(ms, device="cuda")
         dist.barrier()
     return ms, launched, kms, kn
 
@@ -286,7 +284,7 @@ def e2e_steps(s, steps, wl, dist):
     """End to end through the public host-buffer entry point: every step copies the
     inflow profile from pinned host memory and reads the status word back."""
     import torch
-    from lbm_b200 import workloads as W
+    from lbm_b200 import replicas, workloads as W
     uvel_host = torch.from_numpy(W.inflow_profile(wl)).pin_memory()
     if dist is not None:
         dist.barrier()
@@ -298,9 +296,7 @@ def e2e_steps(s, steps, wl, dist):
     torch.cuda.synchronize()
     el = time.perf_counter() - t0
     if dist is not None:
-        t = torch.tensor([el], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el = float(t.item())
+        el = replicas.max_over_ranks(el, device="cuda")
     return el, bad, wl.nz * 4, 4
 
 
@@ -312,19 +308,17 @@ def main():
         return run_reference(a, wl)
 
     import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from lbm_b200 import replicas
+    rank, local, world = replicas.env_rank()
     dist = None
     if world > 1:
-        import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist = replicas.init("nccl", timeout_s=120, device=torch.device("cuda", local))
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    s = make_solver(wl, a.storage, seed=wl.seed + rank)
+    s = make_solver(wl, a.storage, seed=replicas.replica_seed(wl.seed, rank))
     s.step(a.warmup)
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
@@ -361,7 +355,7 @@ def main():
     torch.cuda.empty_cache()
 
     if not a.no_f16 and a.storage == "f32" and world == 1:
-        s16 = make_solver(wl, "f16", seed=wl.seed + rank)
+        s16 = make_solver(wl, "f16", seed=replicas.replica_seed(wl.seed, rank))
         s16.step(a.warmup)
         ms16, _, kms16, kn16 = timed_steps(s16, a.steps, dist)
         s16.close()

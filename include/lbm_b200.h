@@ -55,7 +55,14 @@ enum {
 
 /* status bits returned by lbm_status() */
 enum {
-    LBM_STATUS_BAD_DENSITY = 1   /* some cell had rho <= 0, NaN or Inf (m_rhotest.F90) */
+    LBM_STATUS_BAD_DENSITY = 1,  /* some cell had rho <= 0, NaN or Inf (m_rhotest.F90) */
+    LBM_STATUS_TIMEOUT = 4       /* a pipeline wait in the step kernel gave up (the step is incomplete) */
+};
+
+/* steady step kernel of the fused state (lbm_set_kernel) */
+enum {
+    LBM_KERNEL_TMA = 0,    /* shared-memory tiles filled by bulk copies                      */
+    LBM_KERNEL_PULL = 1    /* direct coalesced global loads, one cell per thread (default)   */
 };
 
 /* Run-time options.  Field meanings follow m_readinfile.F90:3-58 and
@@ -152,12 +159,22 @@ int lbm_set_turbulence(lbm_ctx* ctx, const float* uu, const float* vv, const flo
 int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
 /* advance nsteps time steps */
 int lbm_step(lbm_ctx* ctx, int32_t nsteps);
+/* choose the steady step kernel (LBM_KERNEL_*); both give the same results to round-off */
+int lbm_set_kernel(lbm_ctx* ctx, int32_t which);
 /* host-buffer step: copies uvel(nz) from host memory before each step (NULL keeps the
  * current profile), runs nsteps steps, and writes the status word to *status_host */
 int lbm_step_host(lbm_ctx* ctx, int32_t nsteps, const float* uvel_host, int32_t* status_host);
 int lbm_get_step(lbm_ctx* ctx, int32_t* it);
 /* accumulated LBM_STATUS_* bits since the last call; synchronises and clears them */
 int lbm_status(lbm_ctx* ctx, int32_t* flags);
+
+/* ---- conservation (FP64) ---------------------------------------------------------
+ * Mass sum(rho) and momentum sum(rho u) over the interior cells, accumulated in FP64
+ * (the reference prints averages of rho, u in m_diag.F90; it has no such reduction). */
+/* f: reference-layout device array; out: 4 doubles (mass, mx, my, mz) in device memory */
+int lbm_mass_momentum(lbm_ctx* ctx, const float* f, double* out);
+/* the same for the current fused state (the reference's f1); out_host: 4 doubles, synchronises */
+int lbm_conservation(lbm_ctx* ctx, double* out_host);
 
 /* ---- instrumentation (no counterpart in the reference, whose timers are m_wtime.F90) ---- */
 /* number of kernel launches this context has issued */

@@ -24,6 +24,9 @@ ERR_NAMES = {0: "LBM_OK", -1: "LBM_ERR_ARG", -2: "LBM_ERR_UNSUPPORTED", -3: "LBM
 LBM_STORE_F32 = 0
 LBM_STORE_F16 = 1
 LBM_STATUS_BAD_DENSITY = 1
+LBM_STATUS_TIMEOUT = 4
+LBM_KERNEL_TMA = 0
+LBM_KERNEL_PULL = 1
 
 
 class LbmParams(ctypes.Structure):
@@ -68,9 +71,12 @@ SIGNATURES = {
     "lbm_set_turbulence": [P, P, P, P, I, F],
     "lbm_set_inflow": [P, P],
     "lbm_step": [P, I],
+    "lbm_set_kernel": [P, I],
     "lbm_step_host": [P, I, P, ctypes.POINTER(ctypes.c_int32)],
     "lbm_get_step": [P, ctypes.POINTER(ctypes.c_int32)],
     "lbm_status": [P, ctypes.POINTER(ctypes.c_int32)],
+    "lbm_mass_momentum": [P, P, P],
+    "lbm_conservation": [P, ctypes.POINTER(ctypes.c_double)],
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],

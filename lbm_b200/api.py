@@ -230,6 +230,10 @@ class Lbm:
     def step(self, nsteps=1):
         self._call("lbm_step", ctypes.c_int32(nsteps))
 
+    def set_kernel(self, which: str):
+        """Steady step kernel: "pull" (direct loads, default) or "tma" (shared-memory tiles)."""
+        self._call("lbm_set_kernel", ctypes.c_int32({"tma": _lib.LBM_KERNEL_TMA, "pull": _lib.LBM_KERNEL_PULL}[which]))
+
     def step_host(self, nsteps, uvel_host=None):
         """Steps with host buffers: uvel_host is a CPU float32 tensor (pinned for async copies)."""
         st = ctypes.c_int32(0)
@@ -252,6 +256,22 @@ class Lbm:
 
     def synchronize(self):
         self._call("lbm_synchronize")
+
+    # ---- conservation ----------------------------------------------------------------
+    def mass_momentum(self, f, out=None):
+        """FP64 (mass, mx, my, mz) of a reference-layout f; returns a CUDA float64 tensor of 4."""
+        self._f(f)
+        if out is None:
+            out = torch.zeros(4, dtype=torch.float64, device="cuda")
+        self._chk(out, (4,), torch.float64, name="out")
+        self._call("lbm_mass_momentum", _ptr(f), _ptr(out))
+        return out
+
+    def conservation(self):
+        """FP64 (mass, mx, my, mz) of the fused state's f1."""
+        v = (ctypes.c_double * 4)()
+        self._call("lbm_conservation", v)
+        return tuple(v)
 
     # ---- instrumentation -------------------------------------------------------------
     @property

@@ -1,4 +1,5 @@
 // api.cu -- C ABI of the B200 LBM library (declarations in include/lbm_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -10,10 +11,13 @@
 #include "boundary.cuh"
 #include "ref_kernels.cuh"
 #include "state_kernels.cuh"
+#include "tma_step.cuh"
 
 using namespace lbm;
 
 enum { ST_NONE = 0, ST_PRE = 1, ST_POST = 2 };
+// blocks of the conservation reduction (a few per SM)
+#define LBM_SUM_BLOCKS 1184
 
 struct lbm_ctx {
     lbm_params p;
@@ -43,11 +47,16 @@ struct lbm_ctx {
     bool fold = false;            // boundaries folded into the step kernel (see state_kernels.cuh)
     void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
     bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
+    int kernel = LBM_KERNEL_PULL; // steady step kernel (lbm_set_kernel)
+    int tma_grid[2] = {0, 0};     // persistent grid of k_step_tma per (wrap) variant, 0 = not sized yet
+    int nsm = 148;
     int kopt_lo = 0, kopt_hi = 0;
     float* d_uvel = nullptr;      // uvel(nz)
     float* d_abl = nullptr;       // ablvisc(nz), zero unless set
     int* d_it = nullptr;          // number of the step being computed
     int* d_status = nullptr;
+    double* d_partial = nullptr;  // FP64 block partials of the conservation sums (scratch)
+    double* d_sum = nullptr;      // their total (4 doubles)
     int it = 0;
     // instrumentation: kernel launches issued, optional event timing of the step kernel
     long long launches = 0;
@@ -359,6 +368,27 @@ StepArgs step_args(lbm_ctx* c) {
     return a;
 }
 
+// persistent grid of k_step_tma: resident CTAs per SM x SMs, at most one CTA per tile
+template <int Q, typename S, bool WRAP>
+int tma_launch(lbm_ctx* c, const S* src, S* dst, const StepArgs& a) {
+    const SoaGrid& g = c->sg;
+    const long long ntiles = (long long)((g.nx + kTileCells - 1) / kTileCells) * g.ny * g.nz;
+    const int smem = tma_smem_bytes<Q, S>();
+    int& grid = c->tma_grid[WRAP ? 1 : 0];
+    if (grid == 0) {
+        int occ = 0;
+        LBM_TRY(cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_tma<Q, S, WRAP>, 128, smem),
+                           "occupancy"));
+        if (occ < 1) return fail(c, LBM_ERR_CUDA, "k_step_tma does not fit on an SM");
+        grid = occ * c->nsm;
+    }
+    const int nblk = (int)std::min<long long>(grid, ntiles);
+    k_step_tma<Q, S, WRAP><<<nblk, 128, smem, c->stream>>>(src, dst, a, ntiles);
+    c->launches++;
+    LBM_LAUNCHED(c, "fused step (tma)");
+    return LBM_OK;
+}
+
 template <int Q, typename S>
 int step_one(lbm_ctx* c) {
     const SoaGrid& g = c->sg;
@@ -373,12 +403,16 @@ int step_one(lbm_ctx* c) {
     } else if (c->fold) {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        if (c->idx32)
-            k_step_fast<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-        else
-            k_step<Q, S, true, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-        c->launches++;
-        LBM_LAUNCHED(c, "fused step");
+        if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
+            LBM_TRY(tma_launch<Q, S, true>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
+        } else {
+            if (c->idx32)
+                k_step_fast<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            else
+                k_step<Q, S, true, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            c->launches++;
+            LBM_LAUNCHED(c, "fused step");
+        }
         LBM_TRY(prof_end(c));
         const int nface = 2 * g.ny * ((g.nx + 127) / 128);
         const long long nxg = (long long)Q * g.ny * g.nz;
@@ -392,12 +426,16 @@ int step_one(lbm_ctx* c) {
     } else {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        if (c->idx32)
-            k_step_fast<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-        else
-            k_step<Q, S, true, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-        c->launches++;
-        LBM_LAUNCHED(c, "fused step");
+        if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
+            LBM_TRY(tma_launch<Q, S, false>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
+        } else {
+            if (c->idx32)
+                k_step_fast<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            else
+                k_step<Q, S, true, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            c->launches++;
+            LBM_LAUNCHED(c, "fused step");
+        }
         LBM_TRY(prof_end(c));
         c->cur = nxt;
     }
@@ -440,6 +478,18 @@ void launch_macro(lbm_ctx* c, float* rho, float* u, float* v, float* w) {
     const SoaGrid& g = c->sg;
     k_macro<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(
         (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g, wrap_rows(c));
+    c->launches++;
+}
+
+template <int Q, typename S>
+void launch_sum_state(lbm_ctx* c) {
+    k_sum_state<Q, S><<<LBM_SUM_BLOCKS, 256, 0, c->stream>>>((const S*)c->buf[c->cur], c->sg, wrap_rows(c),
+                                                            c->d_partial);
+    c->launches++;
+}
+template <int Q, typename S>
+void launch_sum_pre(lbm_ctx* c) {
+    k_sum_stored<Q, S><<<LBM_SUM_BLOCKS, 256, 0, c->stream>>>((const S*)c->buf[c->cur], c->sg, c->d_partial);
     c->launches++;
 }
 
@@ -491,8 +541,10 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
         if (rc == LBM_OK && e != cudaSuccess) rc = cuda_check(c, e, w);
     };
     chk(cudaGetDevice(&c->dev), "cudaGetDevice");
+    if (rc == LBM_OK) chk(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev), "cudaDeviceGetAttribute");
     c->stream = nullptr;
-    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem;
+    // + 1 KiB: the bulk copies of k_step_tma read up to ~100 elements past the last row
+    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem + 1024;
     for (int b = 0; b < 2 && rc == LBM_OK; ++b) {
         chk(cudaMalloc(&c->buf[b], nbuf), "cudaMalloc(state)");
         if (rc == LBM_OK) chk(cudaMemset(c->buf[b], 0, nbuf), "cudaMemset(state)");
@@ -504,6 +556,8 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     chk(cudaMalloc(&c->d_abl, (size_t)p->nz * sizeof(float)), "cudaMalloc(ablvisc)");
     chk(cudaMalloc(&c->d_it, 2 * sizeof(int)), "cudaMalloc(step)");
     chk(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc(status)");
+    chk(cudaMalloc(&c->d_partial, (size_t)LBM_SUM_BLOCKS * 4 * sizeof(double)), "cudaMalloc(partial)");
+    chk(cudaMalloc(&c->d_sum, 4 * sizeof(double)), "cudaMalloc(sum)");
     if (rc == LBM_OK) {
         chk(cudaMemset(c->d_uvel, 0, (size_t)p->nz * sizeof(float)), "cudaMemset");
         chk(cudaMemset(c->d_abl, 0, (size_t)p->nz * sizeof(float)), "cudaMemset");
@@ -532,6 +586,8 @@ int lbm_destroy(lbm_ctx* c) {
     cudaFree(c->d_abl);
     cudaFree(c->d_it);
     cudaFree(c->d_status);
+    cudaFree(c->d_partial);
+    cudaFree(c->d_sum);
     delete c;
     return LBM_OK;
 }
@@ -840,6 +896,41 @@ int lbm_step_host(lbm_ctx* c, int32_t nsteps, const float* uvel_host, int32_t* s
 int lbm_get_step(lbm_ctx* c, int32_t* it) {
     if (!c || !it) return LBM_ERR_ARG;
     *it = c->it;
+    return LBM_OK;
+}
+
+int lbm_mass_momentum(lbm_ctx* c, const float* f, double* out) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, out);
+    if (c->p.nl == 27) k_sum_ref<27><<<LBM_SUM_BLOCKS, 256, 0, c->stream>>>(f, c->rg, c->d_partial);
+    else k_sum_ref<19><<<LBM_SUM_BLOCKS, 256, 0, c->stream>>>(f, c->rg, c->d_partial);
+    c->launches++;
+    k_sum_final<<<1, 256, 0, c->stream>>>(c->d_partial, LBM_SUM_BLOCKS, out);
+    c->launches++;
+    LBM_LAUNCHED(c, "mass_momentum");
+    return LBM_OK;
+}
+
+int lbm_conservation(lbm_ctx* c, double* out_host) {
+    if (!c || !out_host) return LBM_ERR_ARG;
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "conservation: no state imported");
+    if (c->state == ST_POST) {
+        DISPATCH_QS(c, launch_sum_state, c);
+    } else {
+        DISPATCH_QS(c, launch_sum_pre, c);
+    }
+    k_sum_final<<<1, 256, 0, c->stream>>>(c->d_partial, LBM_SUM_BLOCKS, c->d_sum);
+    c->launches++;
+    LBM_LAUNCHED(c, "conservation");
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(out_host, c->d_sum, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                       "conservation"));
+    return cuda_check(c, cudaStreamSynchronize(c->stream), "conservation");
+}
+
+int lbm_set_kernel(lbm_ctx* c, int32_t which) {
+    if (!c) return LBM_ERR_ARG;
+    if (which != LBM_KERNEL_TMA && which != LBM_KERNEL_PULL) return fail(c, LBM_ERR_ARG, "set_kernel: unknown kernel");
+    c->kernel = which;
     return LBM_OK;
 }
 

@@ -278,25 +278,13 @@ struct Load32<Q, S, Q> {
     static __device__ __forceinline__ void run(float (&)[Q], const S*, const S*, const S*, const StepArgs&) {}
 };
 
-// Steady fused step with the row-organised collision (collide_rows.cuh).  FP16
-// state is used in its 2^8-scaled form: the moments are rescaled once and the
-// emission constants carry the scale, so no population is multiplied on the way
-// in or out.  Needs Q * dstride < 2^31 (32-bit element offsets).
+// Everything after the loads of one cell of the steady step: moments, collision
+// (regularized rows or the plain BGK of collide.cuh), turbulence slice, solid
+// swap, stores, and the edge copy of the folded boundaries.  fp holds the pulled
+// offsets (2^8-scaled for FP16).
 template <int Q, typename S, bool WRAP>
-__global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src, S* __restrict__ dst, StepArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > a.g.nx) return;
-    const long long o = a.g.off(i, j, k);
-    float fp[Q];
-    {
-        const S* p0 = src + o;
-        const long long wrapd = (long long)a.g.ny * a.g.pitch;
-        const S* pyp = (WRAP && j == 1) ? p0 + wrapd : p0;         // row 0 -> row ny
-        const S* pym = (WRAP && j == a.g.ny) ? p0 - wrapd : p0;    // row ny+1 -> row 1
-        Load32<Q, S, 0>::run(fp, p0, pyp, pym, a);
-    }
+__device__ __forceinline__ void cell_update(float (&fp)[Q], S* __restrict__ dst, const StepArgs& a, int i, int j,
+                                            int k) {
     Moments m = moments_rows<Q>(fp);
     constexpr float inv_scale = 1.0f / store_scale<S>();
     if constexpr (sizeof(S) == 2) {
@@ -326,7 +314,7 @@ __global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src,
 #pragma unroll
         for (int l = 0; l < Q; ++l) fp[l] *= store_scale<S>();
     }
-    S* q = dst + o;
+    S* q = dst + a.g.off(i, j, k);
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
         if constexpr (sizeof(S) == 2) q[a.soff[l]] = __float2half_rn(fp[l]);
@@ -342,6 +330,28 @@ __global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src,
             else e[l * nyz] = fp[l];
         }
     }
+}
+
+// Steady fused step with the row-organised collision (collide_rows.cuh).  FP16
+// state is used in its 2^8-scaled form: the moments are rescaled once and the
+// emission constants carry the scale, so no population is multiplied on the way
+// in or out.  Needs Q * dstride < 2^31 (32-bit element offsets).
+template <int Q, typename S, bool WRAP>
+__global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src, S* __restrict__ dst, StepArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > a.g.nx) return;
+    const long long o = a.g.off(i, j, k);
+    float fp[Q];
+    {
+        const S* p0 = src + o;
+        const long long wrapd = (long long)a.g.ny * a.g.pitch;
+        const S* pyp = (WRAP && j == 1) ? p0 + wrapd : p0;         // row 0 -> row ny
+        const S* pym = (WRAP && j == a.g.ny) ? p0 - wrapd : p0;    // row ny+1 -> row 1
+        Load32<Q, S, 0>::run(fp, p0, pyp, pym, a);
+    }
+    cell_update<Q, S, WRAP>(fp, dst, a, i, j, k);
 }
 
 // Advance the device step counter after the boundary kernels of a step.
@@ -441,6 +451,127 @@ __global__ void __launch_bounds__(128) k_macro(const S* __restrict__ src, const 
     u[c] = m.jx * inv;
     v[c] = m.jy * inv;
     w[c] = m.jz * inv;
+}
+
+}  // namespace lbm
+
+namespace lbm {
+
+// ---------------------------------------------------------------------------
+// FP64 conservation sums: mass sum(rho) and momentum sum(rho u) over the
+// interior cells.  Each cell's moments are formed in FP32 (as macrovars does)
+// and accumulated in FP64; blocks reduce with warp shuffles and write one
+// partial each, a single-block kernel adds the partials in a fixed order.
+// ---------------------------------------------------------------------------
+struct Sum4 {
+    double r, x, y, z;
+};
+
+__device__ __forceinline__ Sum4 warp_sum4(Sum4 s) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        s.r += __shfl_down_sync(0xffffffffu, s.r, o);
+        s.x += __shfl_down_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_down_sync(0xffffffffu, s.y, o);
+        s.z += __shfl_down_sync(0xffffffffu, s.z, o);
+    }
+    return s;
+}
+
+// block reduction of per-thread sums into partial[blockIdx.x*4 .. +3]; blockDim.x = 256
+__device__ __forceinline__ void block_sum4_store(Sum4 s, double* partial) {
+    __shared__ double sm[8][4];
+    s = warp_sum4(s);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sm[w][0] = s.r; sm[w][1] = s.x; sm[w][2] = s.y; sm[w][3] = s.z;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += sm[q][threadIdx.x];
+        partial[blockIdx.x * 4 + threadIdx.x] = t;
+    }
+}
+
+// interior cells of a reference-layout f(nl,0:nx+1,0:ny+1,0:nz+1)
+template <int Q>
+__global__ void __launch_bounds__(256) k_sum_ref(const float* __restrict__ f, RefGrid g, double* partial) {
+    Sum4 s = {0.0, 0.0, 0.0, 0.0};
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long c = blockIdx.x * 256LL + threadIdx.x; c < n; c += (long long)gridDim.x * 256) {
+        const int i = (int)(c % g.nx) + 1;
+        const int j = (int)((c / g.nx) % g.ny) + 1;
+        const int k = (int)(c / ((long long)g.nx * g.ny)) + 1;
+        const float* p = f + g.cell(i, j, k) * Q;
+        float r = 0.f, x = 0.f, y = 0.f, z = 0.f;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            const float v = p[l];
+            r += v;
+            macc(x, lat_cx(l), v);
+            macc(y, lat_cy(l), v);
+            macc(z, lat_cz(l), v);
+        }
+        s.r += r; s.x += x; s.y += y; s.z += z;
+    }
+    block_sum4_store(s, partial);
+}
+
+// interior cells of the reference's f1 of the fused state (pulled from src)
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_sum_state(const S* __restrict__ src, SoaGrid g, int wrap, double* partial) {
+    Sum4 s = {0.0, 0.0, 0.0, 0.0};
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long c = blockIdx.x * 256LL + threadIdx.x; c < n; c += (long long)gridDim.x * 256) {
+        const int i = (int)(c % g.nx) + 1;
+        const int j = (int)((c / g.nx) % g.ny) + 1;
+        const int k = (int)(c / ((long long)g.nx * g.ny)) + 1;
+        float fp[Q];
+        PullMacro<Q, S, 0>::run(fp, src, g, g.off(i, j, k), j, wrap != 0);
+        const Moments m = moments<Q>(fp);
+        s.r += 1.0 + (double)m.s0;     // f = f' + w_l and sum w_l = 1
+        s.x += m.jx; s.y += m.jy; s.z += m.jz;
+    }
+    block_sum4_store(s, partial);
+}
+
+// interior cells of a stored state buffer as it is (an imported f1, before any step)
+template <int Q, typename S>
+__global__ void __launch_bounds__(256) k_sum_stored(const S* __restrict__ src, SoaGrid g, double* partial) {
+    Sum4 s = {0.0, 0.0, 0.0, 0.0};
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    for (long long c = blockIdx.x * 256LL + threadIdx.x; c < n; c += (long long)gridDim.x * 256) {
+        const int i = (int)(c % g.nx) + 1;
+        const int j = (int)((c / g.nx) % g.ny) + 1;
+        const int k = (int)(c / ((long long)g.nx * g.ny)) + 1;
+        float fp[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fp[l] = Store<S>::to_f(src[(long long)l * g.dstride + g.off(i, j, k)]);
+        const Moments m = moments<Q>(fp);
+        s.r += 1.0 + (double)m.s0;
+        s.x += m.jx; s.y += m.jy; s.z += m.jz;
+    }
+    block_sum4_store(s, partial);
+}
+
+__global__ void __launch_bounds__(256) k_sum_final(const double* __restrict__ partial, int nblocks, double* out) {
+    Sum4 s = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nblocks; b += 256) {
+        s.r += partial[b * 4 + 0]; s.x += partial[b * 4 + 1]; s.y += partial[b * 4 + 2]; s.z += partial[b * 4 + 3];
+    }
+    __shared__ double sm[8][4];
+    s = warp_sum4(s);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sm[w][0] = s.r; sm[w][1] = s.x; sm[w][2] = s.y; sm[w][3] = s.z;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int q = 0; q < 8; ++q) t += sm[q][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
 }
 
 }  // namespace lbm

@@ -56,7 +56,7 @@ def run_oracle(wl, steps, dtype, iturb, blank, turb):
     return fA, fB, rho, u, v, w
 
 
-def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32"):
+def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32", kernel="pull"):
     from lbm_b200 import Solver
     rho, u, v, w = (cuda(a) for a in W.initial_macro(wl))
     uvel = cuda(W.inflow_profile(wl))
@@ -65,6 +65,7 @@ def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32"):
         tb = (cuda(turb[0]), cuda(turb[1]), cuda(turb[2]), wl.nrturb, wl.ampl)
     s = Solver(params_of(wl, iturb_pos=iturb, storage=storage), rho, u, v, w, uvel,
                blanking=cuda(blank) if blank is not None else None, turbulence=tb, fused=fused)
+    s.lbm.set_kernel(kernel)
     s.step(steps)
     f1, f2 = s.state()
     r, uu, vv, ww = s.macro()
@@ -112,6 +113,23 @@ def test_small_step_matches_oracle(nl, fused):
     ref32 = run_oracle(wl, wl.steps, np.float32, 5, blank, turb)
     ref64 = run_oracle(wl, wl.steps, np.float64, 5, blank, turb)
     compare_to_floor(gpu, ref32, ref64, "fused" if fused else "per-call")
+
+
+@pytest.mark.parametrize("nl", [19, 27])
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_tma_kernel_matches_pull_kernel(nl, storage):
+    """The shared-memory-tile step kernel gives the pull kernel's results (round-off)."""
+    wl = SMALL.with_(nl=nl, nx=300)        # three tiles per row, the last one partial
+    blank = W.blanking(wl)
+    turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
+    a = run_gpu(wl, 12, 5, blank, turb, storage=storage, kernel="pull")
+    b = run_gpu(wl, 12, 5, blank, turb, storage=storage, kernel="tma")
+    e = errors(b, a)
+    assert all(v < 1e-6 for v in e.values()), e
+    if storage == "f32":
+        ref32 = run_oracle(wl, 12, np.float32, 5, blank, turb)
+        ref64 = run_oracle(wl, 12, np.float64, 5, blank, turb)
+        compare_to_floor(b, ref32, ref64, "tma")
 
 
 @pytest.mark.parametrize("codes", [(11, 22, 12), (22, 21, 11), (12, 11, 22), (0, 0, 0), (1, 11, 22), (0, 12, 0)])
