@@ -176,6 +176,24 @@ int lbm_mass_momentum(lbm_ctx* ctx, const float* f, double* out);
 /* the same for the current fused state (the reference's f1); out_host: 4 doubles, synchronises */
 int lbm_conservation(lbm_ctx* ctx, double* out_host);
 
+/* ---- allocation-free variant (no counterpart in the reference) -------------------------
+ * The same sums as lbm_mass_momentum, for callers that must not allocate device memory:
+ * a host program whose device memory is owned by another runtime's pool or budget (every
+ * byte has to go through that allocator), a monitoring hook inside a solver loop where
+ * the implicit device synchronisation of cudaMalloc/cudaFree is not acceptable, or an
+ * embedder whose only allocator is a fixed arena.  It needs no context (lbm_create
+ * allocates) and calls no cudaMalloc/cudaFree: the per-block
+ * partial sums live in a fixed 64 KiB device array inside the library, so grids are
+ * limited to 134,217,728 interior cells (nx*ny*nz); larger grids return LBM_ERR_ARG.
+ * f: reference-layout device array f(nl,0:nx+1,0:ny+1,0:nz+1); out: 4 doubles
+ * (mass, mx, my, mz) in device memory; stream: cudaStream_t (NULL = legacy default).
+ * The first call on a device looks up the array's device address, so make that call
+ * before any stream capture.  Every call reuses the same array, each block overwriting
+ * its own partial before the final sum reads it: calls that may overlap on the GPU
+ * (different streams, or different host threads) race and must be serialised. */
+int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
+                              void* stream);
+
 /* ---- instrumentation (no counterpart in the reference, whose timers are m_wtime.F90) ---- */
 /* number of kernel launches this context has issued */
 int lbm_launch_count(lbm_ctx* ctx, int64_t* n);

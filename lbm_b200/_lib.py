@@ -77,6 +77,7 @@ SIGNATURES = {
     "lbm_status": [P, ctypes.POINTER(ctypes.c_int32)],
     "lbm_mass_momentum": [P, P, P],
     "lbm_conservation": [P, ctypes.POINTER(ctypes.c_double)],
+    "lbm_mass_momentum_noalloc": [P, I, I, I, I, P, P],
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],

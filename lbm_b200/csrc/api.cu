@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -14,6 +15,17 @@
 #include "tma_step.cuh"
 
 using namespace lbm;
+
+// ---------------------------------------------------------------------------
+// Scratch of lbm_mass_momentum_noalloc: a fixed device array instead of a
+// cudaMalloc'ed buffer.  LBM_NOALLOC_BLOCKS block partials of 4 doubles
+// (64 KiB), one block per LBM_NOALLOC_CHUNK interior cells, so grids of up to
+// 2048 * 65536 = 134,217,728 interior cells.  Every GPU that loads the library
+// holds this array until the process exits.
+// ---------------------------------------------------------------------------
+#define LBM_NOALLOC_BLOCKS 2048
+#define LBM_NOALLOC_CHUNK 65536LL
+static __device__ __align__(256) double g_noalloc_partial[LBM_NOALLOC_BLOCKS * 4];
 
 enum { ST_NONE = 0, ST_PRE = 1, ST_POST = 2 };
 // blocks of the conservation reduction (a few per SM)
@@ -925,6 +937,42 @@ int lbm_conservation(lbm_ctx* c, double* out_host) {
     LBM_TRY(cuda_check(c, cudaMemcpyAsync(out_host, c->d_sum, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
                        "conservation"));
     return cuda_check(c, cudaStreamSynchronize(c->stream), "conservation");
+}
+
+// Device address of g_noalloc_partial on the current device, looked up once per
+// device (host code may not use the symbol itself as an address).
+static int noalloc_scratch(double** out) {
+    static std::mutex mu;
+    static double* addr[128] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return LBM_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_partial) != cudaSuccess || !p) return LBM_ERR_CUDA;
+        addr[dev] = (double*)p;
+    }
+    *out = addr[dev];
+    return LBM_OK;
+}
+
+int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
+                              void* stream) {
+    if (!f || !out) return LBM_ERR_ARG;
+    if (nl != 19 && nl != 27) return LBM_ERR_UNSUPPORTED;
+    if (nx < 1 || ny < 1 || nz < 1) return LBM_ERR_ARG;
+    const long long cells = (long long)nx * ny * nz;
+    const long long nblocks = (cells + LBM_NOALLOC_CHUNK - 1) / LBM_NOALLOC_CHUNK;
+    if (nblocks > LBM_NOALLOC_BLOCKS) return LBM_ERR_ARG;     // more than 134,217,728 interior cells
+    double* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != LBM_OK) return rc;
+    const RefGrid g{nx, ny, nz, nl};
+    cudaStream_t s = (cudaStream_t)stream;
+    if (nl == 27) k_sum_ref<27><<<(int)nblocks, 256, 0, s>>>(f, g, scratch);
+    else k_sum_ref<19><<<(int)nblocks, 256, 0, s>>>(f, g, scratch);
+    k_sum_final<<<1, 256, 0, s>>>(scratch, (int)nblocks, out);
+    return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
 }
 
 int lbm_set_kernel(lbm_ctx* c, int32_t which) {
