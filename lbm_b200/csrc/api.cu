@@ -58,6 +58,7 @@ struct lbm_ctx {
     float ampl = 0.f;
     bool fold = false;            // boundaries folded into the step kernel (see state_kernels.cuh)
     void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
+    void* d_xg[2] = {nullptr, nullptr};  // compact x-ghost columns of each buffer (folded boundaries)
     bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
     int kernel = LBM_KERNEL_PULL; // steady step kernel (lbm_set_kernel)
     int tma_grid[2] = {0, 0};     // persistent grid of k_step_tma per (wrap) variant, 0 = not sized yet
@@ -368,6 +369,7 @@ StepArgs step_args(lbm_ctx* c) {
     a.d_it_rw = c->d_it;
     a.edge = c->d_edge;
     a.full_sector = (c->p.nx % (32 / (int)c->elem)) == 0;
+    a.xg_dst = c->d_xg[1 - c->cur];
     {
         const SoaGrid& g = c->sg;
         const long long plane = (long long)g.pitch * (g.ny + 2);
@@ -399,6 +401,13 @@ int tma_launch(lbm_ctx* c, const S* src, S* dst, const StepArgs& a) {
     c->launches++;
     LBM_LAUNCHED(c, "fused step (tma)");
     return LBM_OK;
+}
+
+template <int Q, typename S>
+void launch_gather_xg(lbm_ctx* c, int b) {
+    const long long n = 2LL * Q * c->sg.ny * c->sg.nz;
+    k_gather_xg<Q, S><<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>((const S*)c->buf[b], (S*)c->d_xg[b], c->sg);
+    c->launches++;
 }
 
 template <int Q, typename S>
@@ -452,6 +461,7 @@ int step_one(lbm_ctx* c) {
         c->cur = nxt;
     }
     LBM_TRY(bc_state<Q, S>(c, c->cur, 1 - c->cur));
+    if (c->fold) launch_gather_xg<Q, S>(c, c->cur);
     k_bump_step<<<1, 32, 0, c->stream>>>(c->d_it);
     c->launches++;
     LBM_LAUNCHED(c, "step counter");
@@ -470,7 +480,11 @@ void launch_import(lbm_ctx* c, const float* ref, int b) {
     const SoaGrid& g = c->sg;
     k_import<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(ref, (S*)c->buf[b], g);
     c->launches++;
+    if (c->fold) launch_gather_xg<Q, S>(c, b);
 }
+// compact x-ghost array of buffer b, or null where the rows hold the x-ghosts
+template <typename S>
+const S* xg_of(const lbm_ctx* c, int b) { return c->fold ? (const S*)c->d_xg[b] : nullptr; }
 // after a step, periodic-j ghost rows are read as rows ny and 1 (state_kernels.cuh)
 int wrap_rows(const lbm_ctx* c) { return (c->state == ST_POST && c->p.jbnd == 0) ? 1 : 0; }
 
@@ -480,16 +494,18 @@ void launch_export(lbm_ctx* c, float* ref, int b, bool pull) {
     dim3 grd((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2);
     if (pull)
         k_export<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], (const S*)c->buf[1 - b], ref, g,
-                                                        wrap_rows(c));
+                                                        wrap_rows(c), xg_of<S>(c, 1 - b));
     else
-        k_export<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], nullptr, ref, g, wrap_rows(c));
+        k_export<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[b], nullptr, ref, g, wrap_rows(c),
+                                                         xg_of<S>(c, b));
     c->launches++;
 }
 template <int Q, typename S>
 void launch_macro(lbm_ctx* c, float* rho, float* u, float* v, float* w) {
     const SoaGrid& g = c->sg;
     k_macro<Q, S><<<dim3((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), 128, 0, c->stream>>>(
-        (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g, wrap_rows(c));
+        (const S*)c->buf[c->cur], (const S*)c->buf[1 - c->cur], rho, u, v, w, g, wrap_rows(c),
+        xg_of<S>(c, 1 - c->cur));
     c->launches++;
 }
 
@@ -565,6 +581,8 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     chk(cudaMalloc(&c->d_macro, 4 * g * sizeof(float)), "cudaMalloc(macro)");
     chk(cudaMalloc(&c->d_uvel, (size_t)p->nz * sizeof(float)), "cudaMalloc(uvel)");
     chk(cudaMalloc(&c->d_edge, (size_t)2 * p->nl * p->ny * p->nz * c->elem), "cudaMalloc(edge)");
+    for (int b = 0; b < 2 && c->fold; ++b)
+        chk(cudaMalloc(&c->d_xg[b], (size_t)2 * p->nl * p->ny * p->nz * c->elem), "cudaMalloc(x-ghost)");
     chk(cudaMalloc(&c->d_abl, (size_t)p->nz * sizeof(float)), "cudaMalloc(ablvisc)");
     chk(cudaMalloc(&c->d_it, 2 * sizeof(int)), "cudaMalloc(step)");
     chk(cudaMalloc(&c->d_status, sizeof(int)), "cudaMalloc(status)");
@@ -595,6 +613,7 @@ int lbm_destroy(lbm_ctx* c) {
     cudaFree(c->d_turb);
     cudaFree(c->d_uvel);
     cudaFree(c->d_edge);
+    for (int b = 0; b < 2; ++b) cudaFree(c->d_xg[b]);
     cudaFree(c->d_abl);
     cudaFree(c->d_it);
     cudaFree(c->d_status);

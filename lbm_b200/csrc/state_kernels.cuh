@@ -20,6 +20,9 @@
 //     reference's ordering (k-faces read x-ghost columns before the inflow
 //     rewrites them) is kept by giving each x-ghost element a single thread
 //     that reads its old value and then writes the new one.
+//   * x-ghost columns (i = 0 and nx+1): each buffer keeps them whole in a
+//     compact array written coalesced by k_bc_fold; the rows hold only the
+//     directions a pull reads (cx > 0 at i = 0, cx < 0 at nx+1).
 #pragma once
 
 #include "collide_rows.cuh"
@@ -51,6 +54,7 @@ struct StepArgs {
     int* d_it_rw;             // step counter, advanced by the boundary kernel
     void* edge;               // post-collision populations at i=1 and i=nx: [side][l][k-1][j-1]
     int full_sector;          // x-ghost sectors hold nothing but the ghost and padding
+    void* xg_dst;             // x-ghost columns of the buffer the step writes: [side][l][k-1][j-1]
     // 32-bit element offsets of k_step_fast, computed on the host:
     int poff[27];             // pull source of direction l relative to the cell: l*dstride - (cx + cy*pitch + cz*plane)
     int soff[27];             // l*dstride
@@ -109,6 +113,12 @@ struct PullLoop<Q, S, Q> {
     static __device__ __forceinline__ void run(float (&)[Q], const S*, const SoaGrid&, long long, int, bool) {}
 };
 
+// Folded configuration: index of ghost (side ? nx+1 : 0, j, k), direction l, in
+// a buffer's compact x-ghost array xg[side][l][k-1][j-1] (j, k interior).
+__device__ __forceinline__ long long xg_index(const SoaGrid& g, int Q, int side, int l, int j, int k) {
+    return ((long long)(side * Q + l) * g.nz + (k - 1)) * g.ny + (j - 1);
+}
+
 // Store one 32-byte sector (two 16-byte vectors) holding v at element `slot`
 // and zeros elsewhere; p is 32-byte aligned.
 template <typename S>
@@ -133,10 +143,12 @@ __device__ __forceinline__ void store_sector(S* p, S v, int slot) {
 //     reflected direction m (m_boundary_k_closed_kernel.F90:157-168).
 //   * x-ghost threads, one per (l, j, k): the inflow value of ghost (0,j,k)
 //     and the outflow value of ghost (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:
-//     184-231).  At the planes k=1 and k=nz they first pass the value their
-//     x-ghost held before this step to the k-ghost cell that the reference's
-//     k-face copies it to (sources i-cx = 0 or nx+1), so each x-ghost element is
-//     read and then written by one and the same thread.
+//     184-231), written to the compact x-ghost array, and into the rows for
+//     the directions the next pull reads there.  At the planes k=1 and k=nz
+//     they first pass the value their x-ghost held before this step to the
+//     k-ghost cell that the reference's k-face copies it to (sources i-cx = 0
+//     or nx+1; always a pulled direction, so it is in the rows), so each
+//     x-ghost element is read and then written by one and the same thread.
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
     const SoaGrid& g = a.g;
@@ -193,18 +205,37 @@ __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a,
     const S gin = Store<S>::from_f(fin - 2.0f * wl * a.rho0 * (cxl * uu * a.cosd + cyl * uu * a.sind) / cs2);
     // outflow: zero gradient
     const S gout = edge[((long long)Q + l) * nyz + cell];
-    S* pin = fl + g.off(0, j, k);
-    S* pout = fl + g.off(g.nx + 1, j, k);
-    if (a.full_sector) {
-        // write each ghost's whole 32-byte sector (the rest is row padding) so the
-        // store needs no read-modify-write of a partial sector
-        constexpr int spe = 32 / (int)sizeof(S);
-        store_sector<S>(pin - (spe - 1), gin, spe - 1);
-        store_sector<S>(pout, gout, 0);
-    } else {
-        *pin = gin;
-        *pout = gout;
+    S* xg = (S*)a.xg_dst;
+    xg[xg_index(g, Q, 0, l, j, k)] = gin;
+    xg[xg_index(g, Q, 1, l, j, k)] = gout;
+    // the rows: a ghost's 32-byte sector holds nothing else but row padding, so
+    // it is written whole (no read-modify-write of a partial sector)
+    constexpr int spe = 32 / (int)sizeof(S);
+    if (cx > 0) {
+        S* p = fl + g.off(0, j, k);
+        if (a.full_sector) store_sector<S>(p - (spe - 1), gin, spe - 1);
+        else *p = gin;
     }
+    if (cx < 0) {
+        S* p = fl + g.off(g.nx + 1, j, k);
+        if (a.full_sector) store_sector<S>(p, gout, 0);
+        else *p = gout;
+    }
+}
+
+// Folded configuration: copy the x-ghost columns of a buffer whose rows hold
+// every direction (after an import or a step with the general boundary
+// kernels) into its compact array.  One thread per element of xg.
+template <int Q, typename S>
+__global__ void __launch_bounds__(128) k_gather_xg(const S* __restrict__ f, S* __restrict__ xg, SoaGrid g) {
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = 2LL * Q * g.ny * g.nz;
+    if (e >= n) return;
+    const int j = (int)(e % g.ny) + 1;
+    const int k = (int)((e / g.ny) % g.nz) + 1;
+    const int l = (int)((e / ((long long)g.ny * g.nz)) % Q);
+    const int side = (int)(e / ((long long)g.ny * g.nz * Q));
+    xg[e] = f[(long long)l * g.dstride + g.off(side ? g.nx + 1 : 0, j, k)];
 }
 
 // PULL = true : dst(interior) = collide(pull(src))        (steady fused step)
@@ -396,10 +427,12 @@ struct PullMacro<Q, S, Q> {
 // State -> reference layout.  PULL: interior cells take the streamed values
 // pulled from `src` (the reference's f1 after drift), ghost cells are copied
 // from `ghost`.  Otherwise every cell is copied from `src`.  wrap: periodic j,
-// ghost rows read from rows ny and 1 (see the file header).
+// ghost rows read from rows ny and 1 (see the file header).  xg: compact
+// x-ghost array of the buffer the ghost cells come from, or null.
 template <int Q, typename S, bool PULL>
 __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const S* __restrict__ ghost,
-                                                float* __restrict__ ref, SoaGrid g, int wrap) {
+                                                float* __restrict__ ref, SoaGrid g, int wrap,
+                                                const S* __restrict__ xg) {
     __shared__ float sm[128 * Q];
     const int i0 = blockIdx.x * 128;
     const int j = blockIdx.y, k = blockIdx.z;
@@ -413,10 +446,13 @@ __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const
         if (PULL && interior) {
             PullMacro<Q, S, 0>::run(v, src, g, g.off(i, j, k), j, wrap != 0);
         } else {
-            const long long o = g.off(i, wrap ? wrapj(j, g.ny) : j, k);
+            const int jw = wrap ? wrapj(j, g.ny) : j;
+            const long long o = g.off(i, jw, k);
             const S* s = PULL ? ghost : src;
+            const bool fromxg = xg && (i == 0 || i == g.nx + 1) && jw >= 1 && jw <= g.ny && k >= 1 && k <= g.nz;
 #pragma unroll
-            for (int l = 0; l < Q; ++l) v[l] = Store<S>::to_f(s[(long long)l * g.dstride + o]);
+            for (int l = 0; l < Q; ++l)
+                v[l] = Store<S>::to_f(fromxg ? xg[xg_index(g, Q, i == 0 ? 0 : 1, l, jw, k)] : s[(long long)l * g.dstride + o]);
         }
 #pragma unroll
         for (int l = 0; l < Q; ++l) sm[t * Q + l] = v[l] + lat_w<Q>(l);
@@ -430,7 +466,8 @@ __global__ void __launch_bounds__(128) k_export(const S* __restrict__ src, const
 // from the pulled values of `src`, ghost cells from `ghost` itself.
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_macro(const S* __restrict__ src, const S* __restrict__ ghost, float* rho,
-                                               float* u, float* v, float* w, SoaGrid g, int wrap) {
+                                               float* u, float* v, float* w, SoaGrid g, int wrap,
+                                               const S* __restrict__ xg) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y, k = blockIdx.z;
     if (i > g.nx + 1) return;
@@ -439,9 +476,12 @@ __global__ void __launch_bounds__(128) k_macro(const S* __restrict__ src, const 
     if (interior) {
         PullMacro<Q, S, 0>::run(fp, src, g, g.off(i, j, k), j, wrap != 0);
     } else {
-        const long long o = g.off(i, wrap ? wrapj(j, g.ny) : j, k);
+        const int jw = wrap ? wrapj(j, g.ny) : j;
+        const long long o = g.off(i, jw, k);
+        const bool fromxg = xg && (i == 0 || i == g.nx + 1) && jw >= 1 && jw <= g.ny && k >= 1 && k <= g.nz;
 #pragma unroll
-        for (int l = 0; l < Q; ++l) fp[l] = Store<S>::to_f(ghost[(long long)l * g.dstride + o]);
+        for (int l = 0; l < Q; ++l)
+            fp[l] = Store<S>::to_f(fromxg ? xg[xg_index(g, Q, i == 0 ? 0 : 1, l, jw, k)] : ghost[(long long)l * g.dstride + o]);
     }
     const Moments m = moments<Q>(fp);
     const float r = 1.0f + m.s0;
