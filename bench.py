@@ -38,9 +38,13 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="turb_inflow_q27_512x256x256")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32")
+    ap.add_argument("--kernel", choices=["pull", "pair", "tma"], default=None,
+                    help="steady step kernel (default: the library's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f16", action="store_true", help="skip the FP16-offset storage comparison")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="FP16-offset storage error study (city workload) instead of the timing run")
     return ap.parse_args()
 
 
@@ -236,7 +240,7 @@ def config_of(wl, storage, n):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def make_solver(wl, storage, seed):
+def make_solver(wl, storage, seed, kernel=None):
     import torch
     from lbm_b200 import Params, Solver, workloads as W
     w2 = wl.with_(seed=seed)
@@ -249,6 +253,8 @@ def make_solver(wl, storage, seed):
     p = Params(nx=w2.nx, ny=w2.ny, nz=w2.nz, nl=w2.nl, ibnd=w2.ibnd, jbnd=w2.jbnd, kbnd=w2.kbnd,
                kinevisc=w2.kinevisc, smagorinsky=w2.smagorinsky, iturb_pos=10, storage=storage)
     s = Solver(p, rho, u, v, w, uvel, blanking=None, turbulence=tb)
+    if kernel is not None:
+        s.lbm.set_kernel(kernel)
     del rho, u, v, w
     torch.cuda.synchronize()
     return s
@@ -300,12 +306,105 @@ def e2e_steps(s, steps, wl, dist):
     return el, bad, wl.nz * 4, 4
 
 
+# ---------------------------------------------------------------------------
+# FP16-offset storage accuracy (the city workload, 1000 steps)
+# ---------------------------------------------------------------------------
+def gpu_run_macro(wl, storage, steps):
+    """rho and (u, v, w) interior fields after `steps` fused steps, as float64 torch tensors."""
+    import torch
+    from lbm_b200 import Params, Solver, workloads as W
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(wl))
+    uvel = torch.from_numpy(W.inflow_profile(wl)).cuda()
+    blank = W.blanking(wl)
+    tb = None
+    if wl.lturb:
+        uu, vv, ww = (torch.from_numpy(x).cuda() for x in W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, wl.seed))
+        tb = (uu, vv, ww, wl.nrturb, wl.ampl)
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd,
+               kinevisc=wl.kinevisc, smagorinsky=wl.smagorinsky, iturb_pos=10, storage=storage)
+    s = Solver(p, rho, u, v, w, uvel, blanking=torch.from_numpy(blank).cuda() if blank is not None else None,
+               turbulence=tb)
+    del rho, u, v, w
+    s.step(steps)
+    r, uu_, vv_, ww_ = s.macro()
+    inner = (slice(1, -1),) * 3
+    out = (r[inner].double(), torch.stack([uu_[inner], vv_[inner], ww_[inner]]).double())
+    st = s.lbm.status()
+    s.close()
+    torch.cuda.synchronize()
+    return out, st
+
+
+def oracle_run_macro(wl, steps, dtype):
+    import numpy as np
+    from lbm_b200 import workloads as W
+    from oracle import oracle as O
+    O.set_threads(cpu_threads())
+    blank = W.blanking(wl)
+    cfg = O.Config(wl.nx, wl.ny, wl.nz, wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=10,
+                   lsolids=blank is not None, lturb=wl.lturb, nrturb=wl.nrturb, ampl=wl.ampl,
+                   kinevisc=wl.kinevisc, smagorinsky=wl.smagorinsky)
+    o = O.Oracle(cfg, dtype)
+    rho, u, v, w = (x.astype(dtype) for x in W.initial_macro(wl))
+    uvel = W.inflow_profile(wl, dtype)
+    fA, fB = o.zeros_f(), o.zeros_f()
+    o.init(fA, fB, rho, u, v, w, uvel)
+    tau = np.full(cfg.sshape, 3 * np.float32(wl.kinevisc) + 0.5, dtype)
+    kw = {}
+    if wl.lturb:
+        kw = {n: x.astype(dtype) for n, x in zip(("uu", "vv", "ww"), W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, wl.seed))}
+    o.run(fA, fB, rho, u, v, w, tau, uvel, steps, blanking=blank, **kw)
+    inner = (slice(1, -1),) * 3
+    return rho[inner].astype(np.float64), np.stack([u[inner], v[inner], w[inner]]).astype(np.float64)
+
+
+def rel_l2_pair(a, b):
+    """relative L2 of rho, of rho - 1 and of the velocity vector field, a against b."""
+    import torch
+    ra, ua = (torch.as_tensor(x, device="cuda", dtype=torch.float64) for x in a)
+    rb, ub = (torch.as_tensor(x, device="cuda", dtype=torch.float64) for x in b)
+    return {"rho": float(torch.linalg.vector_norm(ra - rb) / torch.linalg.vector_norm(rb)),
+            "rho_minus_1": float(torch.linalg.vector_norm(ra - rb) / torch.linalg.vector_norm(rb - 1.0)),
+            "u": float(torch.linalg.vector_norm(ua - ub) / torch.linalg.vector_norm(ub))}
+
+
+def accuracy_study(steps):
+    """FP16-offset storage against plain FP32 on the full city workload, and both
+    against the FP64 oracle (the reference's double-precision build restated) on
+    the reduced city grid, after `steps` steps each."""
+    import torch
+    from lbm_b200 import workloads as W
+    torch.cuda.set_device(0)
+    big, small = W.CITY_Q27, W.CITY_Q27_REDUCED
+    t0 = time.perf_counter()
+    f32, s32 = gpu_run_macro(big, "f32", steps)
+    f16, s16 = gpu_run_macro(big, "f16", steps)
+    full = rel_l2_pair(f16, f32)
+    del f32, f16
+    torch.cuda.empty_cache()
+    r32, _ = gpu_run_macro(small, "f32", steps)
+    r16, _ = gpu_run_macro(small, "f16", steps)
+    t1 = time.perf_counter()
+    ref64 = oracle_run_macro(small, steps, __import__("numpy").float64)
+    t2 = time.perf_counter()
+    line = {"study": "fp16_offset_storage_accuracy", "steps": steps,
+            "full": {"workload": big.name, "f16_vs_f32": full, "status_flags": [s32, s16]},
+            "reduced": {"workload": small.name, "f16_vs_f64_oracle": rel_l2_pair(r16, ref64),
+                        "f32_vs_f64_oracle": rel_l2_pair(r32, ref64), "f16_vs_f32": rel_l2_pair(r16, r32),
+                        "oracle": "C++ restatement in double precision, %d host threads, %.0f s" % (cpu_threads(), t2 - t1)},
+            "bound": "relative L2 <= 1e-3 vs FP64", "gpu_s": round(t1 - t0, 1)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     from lbm_b200 import workloads as W
     wl = W.WORKLOADS[a.workload]
     if a.impl == "reference":
         return run_reference(a, wl)
+    if a.accuracy:
+        return accuracy_study(a.steps)
 
     import torch
     from lbm_b200 import replicas
@@ -318,7 +417,7 @@ def main():
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
 
-    s = make_solver(wl, a.storage, seed=replicas.replica_seed(wl.seed, rank))
+    s = make_solver(wl, a.storage, seed=replicas.replica_seed(wl.seed, rank), kernel=a.kernel)
     s.step(a.warmup)
     torch.cuda.synchronize()
     with ClockSampler(dev) as clk:
@@ -330,7 +429,8 @@ def main():
     bl = bytes_per_lup(wl.nl, a.storage)
     k_ms = kms / max(kn, 1)
     achieved = cells * bl / (k_ms * 1e-3) / 1e9 if kn else None
-    key = "k_step_fast<%d,%s>" % (wl.nl, "float" if a.storage == "f32" else "__half")
+    key = "%s<%d,%s>" % ("k_step_fast" if a.kernel == "pull" else "k_step_pair", wl.nl,
+                         "float" if a.storage == "f32" else "__half")
     traffic = ncu_traffic(key, cells)
     line = {"metric": METRIC, "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "weak",
@@ -355,7 +455,7 @@ def main():
     torch.cuda.empty_cache()
 
     if not a.no_f16 and a.storage == "f32" and world == 1:
-        s16 = make_solver(wl, "f16", seed=replicas.replica_seed(wl.seed, rank))
+        s16 = make_solver(wl, "f16", seed=replicas.replica_seed(wl.seed, rank), kernel=a.kernel)
         s16.step(a.warmup)
         ms16, _, kms16, kn16 = timed_steps(s16, a.steps, dist)
         s16.close()

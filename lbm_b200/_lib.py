@@ -27,6 +27,7 @@ LBM_STATUS_BAD_DENSITY = 1
 LBM_STATUS_TIMEOUT = 4
 LBM_KERNEL_TMA = 0
 LBM_KERNEL_PULL = 1
+LBM_KERNEL_PAIR = 2
 
 
 class LbmParams(ctypes.Structure):

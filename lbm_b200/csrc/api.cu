@@ -13,6 +13,7 @@
 #include "ref_kernels.cuh"
 #include "state_kernels.cuh"
 #include "tma_step.cuh"
+#include "pair_step.cuh"
 
 using namespace lbm;
 
@@ -60,7 +61,7 @@ struct lbm_ctx {
     void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
     void* d_xg[2] = {nullptr, nullptr};  // compact x-ghost columns of each buffer (folded boundaries)
     bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
-    int kernel = LBM_KERNEL_PULL; // steady step kernel (lbm_set_kernel)
+    int kernel = LBM_KERNEL_PAIR; // steady step kernel (lbm_set_kernel); PULL where PAIR does not apply
     int tma_grid[2] = {0, 0};     // persistent grid of k_step_tma per (wrap) variant, 0 = not sized yet
     int nsm = 148;
     int kopt_lo = 0, kopt_hi = 0;
@@ -410,6 +411,11 @@ void launch_gather_xg(lbm_ctx* c, int b) {
     c->launches++;
 }
 
+// the two-cells-per-thread kernel (pair_step.cuh) covers the regularized collision on even nx
+bool pair_shape_ok(const lbm_ctx* c) { return c->idx32 && c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
+bool pair_ok(const lbm_ctx* c) { return c->kernel == LBM_KERNEL_PAIR && pair_shape_ok(c); }
+dim3 pair_grid(const lbm_ctx* c) { return dim3((unsigned)((c->p.nx / 2 + 127) / 128), c->p.ny, c->p.nz); }
+
 template <int Q, typename S>
 int step_one(lbm_ctx* c) {
     const SoaGrid& g = c->sg;
@@ -426,6 +432,10 @@ int step_one(lbm_ctx* c) {
         LBM_TRY(prof_begin(c));
         if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
             LBM_TRY(tma_launch<Q, S, true>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
+        } else if (pair_ok(c)) {
+            k_step_pair<Q, S, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            c->launches++;
+            LBM_LAUNCHED(c, "fused step (pair)");
         } else {
             if (c->idx32)
                 k_step_fast<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
@@ -449,6 +459,10 @@ int step_one(lbm_ctx* c) {
         LBM_TRY(prof_begin(c));
         if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
             LBM_TRY(tma_launch<Q, S, false>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
+        } else if (pair_ok(c)) {
+            k_step_pair<Q, S, false><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            c->launches++;
+            LBM_LAUNCHED(c, "fused step (pair)");
         } else {
             if (c->idx32)
                 k_step_fast<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
@@ -996,7 +1010,8 @@ int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz
 
 int lbm_set_kernel(lbm_ctx* c, int32_t which) {
     if (!c) return LBM_ERR_ARG;
-    if (which != LBM_KERNEL_TMA && which != LBM_KERNEL_PULL) return fail(c, LBM_ERR_ARG, "set_kernel: unknown kernel");
+    if (which != LBM_KERNEL_TMA && which != LBM_KERNEL_PULL && which != LBM_KERNEL_PAIR)
+        return fail(c, LBM_ERR_ARG, "set_kernel: unknown kernel");
     c->kernel = which;
     return LBM_OK;
 }

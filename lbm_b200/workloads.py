@@ -53,7 +53,14 @@ CHANNEL_Q19 = CHANNEL_Q27.with_(name="turb_inflow_q19_512x256x256", nl=19)
 CHANNEL_Q27_SMALL = CHANNEL_Q27.with_(name="turb_inflow_q27_256x128x128", nx=256, ny=128, nz=128)
 CHANNEL_Q19_SMALL = CHANNEL_Q27_SMALL.with_(name="turb_inflow_q19_256x128x128", nl=19)
 
-WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL)}
+# FP16-offset storage study: the channel plus a seeded city of 16 solid boxes on
+# the bottom wall (heights 10-40 cells), and the same city physics on a grid
+# small enough for 1000 steps of the FP64 oracle on the host
+CITY_Q27 = CHANNEL_Q27.with_(name="city_q27_512x256x256", city=16)
+CITY_Q27_REDUCED = CITY_Q27.with_(name="city_q27_128x64x64", nx=128, ny=64, nz=64)
+
+WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL,
+                                 CITY_Q27, CITY_Q27_REDUCED)}
 
 
 def initial_macro(wl: Workload, dtype=np.float32):

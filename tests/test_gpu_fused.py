@@ -56,7 +56,7 @@ def run_oracle(wl, steps, dtype, iturb, blank, turb):
     return fA, fB, rho, u, v, w
 
 
-def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32", kernel="pull"):
+def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32", kernel=None):
     from lbm_b200 import Solver
     rho, u, v, w = (cuda(a) for a in W.initial_macro(wl))
     uvel = cuda(W.inflow_profile(wl))
@@ -65,7 +65,8 @@ def run_gpu(wl, steps, iturb, blank, turb, fused=True, storage="f32", kernel="pu
         tb = (cuda(turb[0]), cuda(turb[1]), cuda(turb[2]), wl.nrturb, wl.ampl)
     s = Solver(params_of(wl, iturb_pos=iturb, storage=storage), rho, u, v, w, uvel,
                blanking=cuda(blank) if blank is not None else None, turbulence=tb, fused=fused)
-    s.lbm.set_kernel(kernel)
+    if kernel is not None:
+        s.lbm.set_kernel(kernel)
     s.step(steps)
     f1, f2 = s.state()
     r, uu, vv, ww = s.macro()
@@ -132,12 +133,45 @@ def test_tma_kernel_matches_pull_kernel(nl, storage):
         compare_to_floor(b, ref32, ref64, "tma")
 
 
+@pytest.mark.parametrize("nl", [19, 27])
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("iturb", [5, 6])
+@pytest.mark.parametrize("kernel", ["pair"])
+def test_pair_kernel_matches_oracle(nl, storage, iturb, kernel):
+    """Two cells per thread (packed f32x2 arithmetic).  FP32: same results as the
+    one-cell kernel to round-off and as close to the oracles as the FP32 floor
+    allows.  FP16 storage: as close to the FP64 oracle as the one-cell kernel
+    (the two differ by FP16 rounding of slightly different FP32 values, so they
+    are compared through their distance to FP64, not to each other).
+    iturb 5 / 6 put the turbulence slice on the first / second cell of a pair."""
+    wl = SMALL.with_(nl=nl)
+    blank = W.blanking(wl)
+    turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
+    a = run_gpu(wl, wl.steps, iturb, blank, turb, storage=storage, kernel="pull")
+    b = run_gpu(wl, wl.steps, iturb, blank, turb, storage=storage, kernel=kernel)
+    check_pair_result(wl, wl.steps, iturb, blank, turb, storage, a, b, kernel)
+
+
+def check_pair_result(wl, steps, iturb, blank, turb, storage, a, b, what):
+    ref64 = run_oracle(wl, steps, np.float64, iturb, blank, turb)
+    if storage == "f32":
+        e = errors(b, a)
+        assert all(v < 1e-6 for v in e.values()), e
+        ref32 = run_oracle(wl, steps, np.float32, iturb, blank, turb)
+        compare_to_floor(b, ref32, ref64, what)
+    else:
+        ea, eb = errors(a, ref64), errors(b, ref64)
+        bad = {k: (eb[k], ea[k]) for k in ea if not eb[k] <= 1.25 * ea[k] + 1e-7}
+        assert not bad, "%s vs FP64 worse than the one-cell kernel: %s" % (what, bad)
+
+
 @pytest.mark.parametrize("codes", [(11, 22, 12), (22, 21, 11), (12, 11, 22), (0, 0, 0), (1, 11, 22), (0, 12, 0)])
 @pytest.mark.parametrize("nl", [19, 27])
-def test_boundary_codes_fused(codes, nl):
+@pytest.mark.parametrize("kernel", ["pull", "pair"])
+def test_boundary_codes_fused(codes, nl, kernel):
     ib, jb, kb = codes
     wl = W.Workload("bc", 10, 8, 6, nl, steps=8, ibnd=ib, jbnd=jb, kbnd=kb, noise=3e-3)
-    gpu = run_gpu(wl, wl.steps, 3, None, None)
+    gpu = run_gpu(wl, wl.steps, 3, None, None, kernel=kernel)
     ref32 = run_oracle(wl, wl.steps, np.float32, 3, None, None)
     ref64 = run_oracle(wl, wl.steps, np.float64, 3, None, None)
     compare_to_floor(gpu, ref32, ref64, "bc %s" % (codes,))
