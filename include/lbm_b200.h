@@ -196,6 +196,43 @@ int lbm_conservation(lbm_ctx* ctx, double* out_host);
 int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
                               void* stream);
 
+/* ---- batched ensemble ----
+ * No counterpart in the reference, which runs one domain per process (main.F90).
+ * An ensemble holds many independent members of different sizes, each an
+ * ordinary context created by the ensemble: import, inflow, turbulence fields,
+ * export and macro reads go through the per-member entry points above on the
+ * context lbm_ensemble_member returns.  lbm_ensemble_step advances every member
+ * together with two launches per step for the whole ensemble (one step kernel,
+ * one boundary kernel), replayed from a CUDA graph of LBM_ENS_GRAPH_STEPS steps
+ * on the ensemble's own stream; the work is ordered after earlier work on, and
+ * before later work on, member 0's stream.  Members need the folded
+ * configuration (ibnd = 1, jbnd = 0, kbnd in {11,12,21,22}), ihrr = 1, an even
+ * nx >= 4, and one lattice and storage for all. */
+typedef struct lbm_ensemble lbm_ensemble;
+enum {
+    LBM_ENS_VARIANTS = 3,      /* launch shapes of the step kernel: 64, 128, 256 threads per block */
+    LBM_ENS_GRAPH_STEPS = 16   /* steps per captured graph (default; lbm_ensemble_set_graph)       */
+};
+int lbm_ensemble_create(lbm_ensemble** ens, const lbm_params* members, int32_t nmembers);
+int lbm_ensemble_destroy(lbm_ensemble* ens);
+/* with ens = NULL: why the calling thread's last lbm_ensemble_create failed */
+const char* lbm_ensemble_last_error(const lbm_ensemble* ens);
+int lbm_ensemble_size(const lbm_ensemble* ens, int32_t* nmembers);
+/* member m's context (owned by the ensemble; do not lbm_destroy it) */
+int lbm_ensemble_member(lbm_ensemble* ens, int32_t m, lbm_ctx** ctx);
+/* advance every member by nsteps.  Members imported since their last step take
+ * their first step alone; all members must be imported before the first call
+ * and afterwards be stepped only through the ensemble. */
+int lbm_ensemble_step(lbm_ensemble* ens, int32_t nsteps);
+/* time each launch shape over trial_steps steps and keep the fastest.  This
+ * advances every member by LBM_ENS_VARIANTS * (trial_steps + 1) steps, plus the
+ * first step of members imported since their last step.  variant and
+ * ms_per_step[LBM_ENS_VARIANTS] may be NULL. */
+int lbm_ensemble_autotune(lbm_ensemble* ens, int32_t trial_steps, int32_t* variant, float* ms_per_step);
+int lbm_ensemble_set_variant(lbm_ensemble* ens, int32_t variant);
+/* steps per captured graph: 0 = direct launches, else a positive even count */
+int lbm_ensemble_set_graph(lbm_ensemble* ens, int32_t graph_steps);
+
 /* ---- instrumentation (no counterpart in the reference, whose timers are m_wtime.F90) ---- */
 /* number of kernel launches this context has issued */
 int lbm_launch_count(lbm_ctx* ctx, int64_t* n);

@@ -28,6 +28,9 @@ LBM_STATUS_TIMEOUT = 4
 LBM_KERNEL_TMA = 0
 LBM_KERNEL_PULL = 1
 LBM_KERNEL_PAIR = 2
+LBM_ENS_VARIANTS = 3
+LBM_ENS_GRAPH_STEPS = 16
+ENS_THREADS = (64, 128, 256)      # threads per block of each ensemble launch shape
 
 
 class LbmParams(ctypes.Structure):
@@ -82,6 +85,14 @@ SIGNATURES = {
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],
+    "lbm_ensemble_create": [ctypes.POINTER(P), ctypes.POINTER(LbmParams), I],
+    "lbm_ensemble_destroy": [P],
+    "lbm_ensemble_size": [P, ctypes.POINTER(ctypes.c_int32)],
+    "lbm_ensemble_member": [P, I, ctypes.POINTER(P)],
+    "lbm_ensemble_step": [P, I],
+    "lbm_ensemble_autotune": [P, I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
+    "lbm_ensemble_set_variant": [P, I],
+    "lbm_ensemble_set_graph": [P, I],
 }
 
 _lib = None
@@ -102,6 +113,8 @@ def load():
         fn.restype = ctypes.c_int32
     lib.lbm_last_error.argtypes = [P]
     lib.lbm_last_error.restype = ctypes.c_char_p
+    lib.lbm_ensemble_last_error.argtypes = [P]
+    lib.lbm_ensemble_last_error.restype = ctypes.c_char_p
     _lib = lib
     return lib
 

@@ -67,23 +67,28 @@ def _ptr(t):
 class Lbm:
     """One context of the C library (``lbm_create``) bound to the current CUDA device."""
 
-    def __init__(self, params: Params, stream: torch.cuda.Stream | None = None):
+    def __init__(self, params: Params, stream: torch.cuda.Stream | None = None, _borrowed=None):
         if not torch.cuda.is_available():
             raise RuntimeError("lbm_b200 needs a CUDA device; there is no CPU fallback")
         self.p = params
         self.L = _lib.load()
         self._cp = params.c()
-        h = ctypes.c_void_p()
-        rc = self.L.lbm_create(ctypes.byref(h), ctypes.byref(self._cp))
-        if rc != 0:
-            raise LbmError(rc, "lbm_create failed for %s" % (params,))
-        self.h = h
+        self._owned = _borrowed is None
+        if _borrowed is not None:      # a member context owned by an Ensemble
+            self.h = _borrowed
+        else:
+            h = ctypes.c_void_p()
+            rc = self.L.lbm_create(ctypes.byref(h), ctypes.byref(self._cp))
+            if rc != 0:
+                raise LbmError(rc, "lbm_create failed for %s" % (params,))
+            self.h = h
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         self._call("lbm_set_stream", ctypes.c_void_p(self.stream.cuda_stream))
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.lbm_destroy(self.h)
+            if self._owned:
+                self.L.lbm_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -290,3 +295,61 @@ class Lbm:
         ms, n = ctypes.c_double(), ctypes.c_int64()
         self._call("lbm_profile_read", ctypes.byref(ms), ctypes.byref(n))
         return ms.value, n.value
+
+
+class Ensemble:
+    """Many independent runs advanced together (``lbm_ensemble_*``): two launches
+    per step for the whole ensemble, replayed from a CUDA graph.  ``members[m]``
+    is an :class:`Lbm` on member m's context, for import, inflow, turbulence,
+    export and macro reads."""
+
+    def __init__(self, params: list[Params], stream: torch.cuda.Stream | None = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("lbm_b200 needs a CUDA device; there is no CPU fallback")
+        self.L = _lib.load()
+        arr = (LbmParams * len(params))(*[p.c() for p in params])
+        h = ctypes.c_void_p()
+        rc = self.L.lbm_ensemble_create(ctypes.byref(h), arr, len(params))
+        if rc != 0:
+            raise LbmError(rc, self.L.lbm_ensemble_last_error(None).decode())
+        self.h = h
+        self.members = []
+        for m, p in enumerate(params):
+            c = ctypes.c_void_p()
+            self._call("lbm_ensemble_member", m, ctypes.byref(c))
+            self.members.append(Lbm(p, stream=stream, _borrowed=c))
+
+    def _call(self, name, *args):
+        rc = getattr(self.L, name)(self.h, *args)
+        if rc != 0:
+            raise LbmError(rc, self.L.lbm_ensemble_last_error(self.h).decode())
+        return rc
+
+    def step(self, nsteps: int = 1):
+        self._call("lbm_ensemble_step", int(nsteps))
+
+    def autotune(self, trial_steps: int = 5):
+        """Time each launch shape; returns (chosen variant, ms per step of each)."""
+        v = ctypes.c_int32(0)
+        ms = (ctypes.c_float * _lib.LBM_ENS_VARIANTS)()
+        self._call("lbm_ensemble_autotune", int(trial_steps), ctypes.byref(v), ms)
+        return v.value, list(ms)
+
+    def set_variant(self, v: int):
+        self._call("lbm_ensemble_set_variant", int(v))
+
+    def set_graph(self, steps: int):
+        self._call("lbm_ensemble_set_graph", int(steps))
+
+    def close(self):
+        if getattr(self, "h", None):
+            for mem in self.members:
+                mem.h = None
+            self.L.lbm_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1052,3 +1052,5 @@ int lbm_status(lbm_ctx* c, int32_t* flags) {
 }
 
 }  // extern "C"
+
+#include "ensemble_host.cuh"

@@ -1,0 +1,86 @@
+// ensemble.cuh -- one launch per phase for a whole ensemble of independent runs.
+//
+// An ensemble is a set of members of different sizes, each a complete fused
+// state (its own buffers, boundaries, inflow, turbulence fields and step
+// counter) in the folded configuration.  The step of every member runs in one
+// launch of k_ens_step and the boundaries of every member in one launch of
+// k_ens_bc.  The blocks of a launch are dealt out member by member: member m
+// owns blocks prefix[m] .. prefix[m+1]-1, so a block never straddles two
+// members.  A block finds its member by a binary search over the prefix table,
+// copies that member's StepArgs into shared memory and then runs the same
+// per-pair (pair_cell) or per-block (bc_fold_block) code as the single-state
+// kernels, so a member of an ensemble computes exactly what it computes alone.
+//
+// In k_ens_step a block of T threads covers T consecutive pairs of the
+// member's pairs flattened row by row (pair q: i = 2 (q mod nx/2) + 1, row
+// q div nx/2), so rows shorter than a block leave no threads idle.
+#pragma once
+
+#include "pair_step.cuh"
+
+namespace lbm {
+
+struct EnsMember {
+    StepArgs a[2];       // arguments of a step whose source is buffer p (p = parity)
+    void* buf[2];
+    int nface_blocks;    // k_bc_fold layout of this member (blocks of 128 threads)
+};
+
+struct EnsLayout {
+    const EnsMember* mem;
+    const int* prefix;   // [nm + 1] first block of each member in this launch's grid
+    int nm;
+};
+
+// member owning block b: the largest m with prefix[m] <= b
+__device__ __forceinline__ int ens_member_of(const int* prefix, int nm, int b) {
+    int lo = 0, hi = nm;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(prefix + mid) <= b) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// the member's arguments into shared memory (word copy; StepArgs is 8-byte aligned)
+__device__ __forceinline__ void ens_load_args(unsigned char* raw, const StepArgs* ga) {
+    constexpr int n = (int)(sizeof(StepArgs) / 4);
+    for (int w = threadIdx.x; w < n; w += blockDim.x)
+        reinterpret_cast<int*>(raw)[w] = __ldg(reinterpret_cast<const int*>(ga) + w);
+    __syncthreads();
+}
+
+template <int Q, typename S, int T, int MINB>
+__global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
+    __shared__ __align__(16) unsigned char raw[sizeof(StepArgs)];
+    const int b = blockIdx.x;
+    const int m = ens_member_of(L.prefix, L.nm, b);
+    const EnsMember* em = L.mem + m;
+    ens_load_args(raw, &em->a[parity]);
+    const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
+    const int hp = a.g.nx / 2;
+    const long long q = (long long)(b - __ldg(L.prefix + m)) * T + threadIdx.x;
+    if (q >= (long long)hp * a.g.ny * a.g.nz) return;
+    const int row = (int)(q / hp);
+    const int i = 2 * (int)(q - (long long)row * hp) + 1;
+    const int j = row % a.g.ny + 1;
+    const int k = row / a.g.ny + 1;
+    const S* src = reinterpret_cast<const S*>(em->buf[parity]);
+    S* dst = reinterpret_cast<S*>(em->buf[1 - parity]);
+    pair_cell<Q, S, true>(src, dst, a, i, j, k);
+}
+
+template <int Q, typename S>
+__global__ void __launch_bounds__(128) k_ens_bc(EnsLayout L, int parity) {
+    __shared__ __align__(16) unsigned char raw[sizeof(StepArgs)];
+    const int b = blockIdx.x;
+    const int m = ens_member_of(L.prefix, L.nm, b);
+    const EnsMember* em = L.mem + m;
+    ens_load_args(raw, &em->a[parity]);
+    const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
+    bc_fold_block<Q, S>(reinterpret_cast<S*>(em->buf[1 - parity]), reinterpret_cast<const S*>(em->buf[parity]), a,
+                        em->nface_blocks, b - __ldg(L.prefix + m));
+}
+
+}  // namespace lbm

@@ -1,0 +1,349 @@
+// ensemble_host.cuh -- C ABI of the batched ensemble (declarations in
+// include/lbm_b200.h).  Included at the end of api.cu, whose lbm_ctx and
+// helpers it uses.
+//
+// The members are ordinary contexts (lbm_create), so every per-member entry
+// point (import, export, set_inflow, set_turbulence, get_macro, ...) applies to
+// them.  lbm_ensemble_step advances all of them together: two launches per step
+// (k_ens_step, k_ens_bc) on the ensemble's own stream, replayed from a CUDA
+// graph of LBM_ENS_GRAPH_STEPS steps when the step count allows.
+
+#include "ensemble.cuh"
+
+namespace {
+
+// launch shapes the autotuner chooses from: threads per block of k_ens_step
+constexpr int kEnsThreads[LBM_ENS_VARIANTS] = {64, 128, 256};
+
+// why the last lbm_ensemble_create of this thread failed (it returns no handle)
+thread_local std::string g_create_err;
+
+}  // namespace
+
+struct lbm_ensemble {
+    std::vector<lbm_ctx*> m;
+    int nl = 19;
+    int storage = LBM_STORE_F32;
+    cudaStream_t stream = nullptr;   // own non-blocking stream (graphs cannot capture the legacy stream)
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    EnsMember* d_mem = nullptr;
+    std::vector<EnsMember> h_mem;
+    int* d_prefix = nullptr;         // [LBM_ENS_VARIANTS + 1][nm + 1]: step grids per variant, then the boundary grid
+    int nblk[LBM_ENS_VARIANTS + 1] = {0, 0, 0, 0};
+    int variant = 1;
+    int graph_steps = LBM_ENS_GRAPH_STEPS;
+    cudaGraphExec_t graph = nullptr;
+    int graph_variant = -1;
+    int cur = 0;
+    std::string err;
+};
+
+namespace {
+
+int efail(lbm_ensemble* e, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (e) e->err = buf;
+    return code;
+}
+int echeck(lbm_ensemble* e, cudaError_t r, const char* what) {
+    if (r == cudaSuccess) return LBM_OK;
+    return efail(e, r == cudaErrorMemoryAllocation ? LBM_ERR_OOM : LBM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(r));
+}
+// a member's error, reported as the ensemble's
+int emember(lbm_ensemble* e, int m, int rc) {
+    if (rc == LBM_OK) return rc;
+    return efail(e, rc, "member %d: %s", m, e->m[m]->err.c_str());
+}
+
+EnsLayout ens_layout(const lbm_ensemble* e, int which) {
+    EnsLayout L;
+    L.mem = e->d_mem;
+    L.prefix = e->d_prefix + (size_t)which * (e->m.size() + 1);
+    L.nm = (int)e->m.size();
+    return L;
+}
+
+// descriptors of every member for both parities (the members' settings may have
+// changed since the last call)
+int ens_upload(lbm_ensemble* e) {
+    for (size_t k = 0; k < e->m.size(); ++k) {
+        lbm_ctx* c = e->m[k];
+        EnsMember& d = e->h_mem[k];
+        const int keep = c->cur;
+        for (int p = 0; p < 2; ++p) {
+            c->cur = p;
+            d.a[p] = step_args(c);
+        }
+        c->cur = keep;
+        d.buf[0] = c->buf[0];
+        d.buf[1] = c->buf[1];
+        d.nface_blocks = 2 * c->sg.ny * ((c->sg.nx + 127) / 128);
+    }
+    return echeck(e, cudaMemcpyAsync(e->d_mem, e->h_mem.data(), e->h_mem.size() * sizeof(EnsMember),
+                                     cudaMemcpyHostToDevice, e->stream), "ensemble descriptors");
+}
+
+template <int Q, typename S>
+int ens_launch_step(lbm_ensemble* e, int parity) {
+    const EnsLayout Ls = ens_layout(e, e->variant);
+    const int nb = e->nblk[e->variant];
+    switch (kEnsThreads[e->variant]) {
+        case 64: k_ens_step<Q, S, 64, 10><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
+        case 128: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        default: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
+    }
+    LBM_TRY(echeck(e, cudaPeekAtLastError(), "ensemble step"));
+    k_ens_bc<Q, S><<<e->nblk[LBM_ENS_VARIANTS], 128, 0, e->stream>>>(ens_layout(e, LBM_ENS_VARIANTS), parity);
+    return echeck(e, cudaPeekAtLastError(), "ensemble boundaries");
+}
+
+int ens_launch(lbm_ensemble* e, int parity) {
+    const bool h = e->storage == LBM_STORE_F16;
+    if (e->nl == 27) return h ? ens_launch_step<27, __half>(e, parity) : ens_launch_step<27, float>(e, parity);
+    return h ? ens_launch_step<19, __half>(e, parity) : ens_launch_step<19, float>(e, parity);
+}
+
+int ens_graph(lbm_ensemble* e) {
+    if (e->graph && e->graph_variant == e->variant) return LBM_OK;
+    if (e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    LBM_TRY(echeck(e, cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "graph capture"));
+    int rc = LBM_OK;
+    for (int s = 0; s < e->graph_steps && rc == LBM_OK; ++s) rc = ens_launch(e, s & 1);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc != LBM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    LBM_TRY(echeck(e, ce, "graph capture"));
+    const cudaError_t ie = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    LBM_TRY(echeck(e, ie, "graph instantiate"));
+    e->graph_variant = e->variant;
+    return LBM_OK;
+}
+
+// members still holding an imported (pre-collision) state take their first step
+// alone (collide in place); afterwards every member must sit on the same buffer
+int ens_align(lbm_ensemble* e, int* used) {
+    *used = 0;
+    bool pre = false;
+    for (size_t k = 0; k < e->m.size(); ++k) {
+        lbm_ctx* c = e->m[k];
+        if (c->state == ST_NONE) return efail(e, LBM_ERR_STATE, "member %d: no state imported", (int)k);
+        if (c->state == ST_PRE) {
+            LBM_TRY(emember(e, (int)k, step_dispatch(c)));
+            pre = true;
+        }
+    }
+    if (pre) *used = 1;
+    for (size_t k = 0; k < e->m.size(); ++k)
+        if (e->m[k]->state != ST_POST || e->m[k]->cur != e->m[0]->cur)
+            return efail(e, LBM_ERR_STATE, "member %d is not at the same step phase as member 0 "
+                         "(import all members, then step them only through the ensemble)", (int)k);
+    e->cur = e->m[0]->cur;
+    return LBM_OK;
+}
+
+// n batched steps on the ensemble stream, ordered after and before the members' stream
+int ens_run(lbm_ensemble* e, int n, bool allow_graph) {
+    cudaStream_t ms = e->m[0]->stream;
+    LBM_TRY(echeck(e, cudaEventRecord(e->ev[0], ms), "ensemble order"));
+    LBM_TRY(echeck(e, cudaStreamWaitEvent(e->stream, e->ev[0], 0), "ensemble order"));
+    LBM_TRY(ens_upload(e));
+    int left = n;
+    while (left > 0) {
+        if (allow_graph && e->graph_steps > 0 && e->cur == 0 && left >= e->graph_steps) {
+            LBM_TRY(ens_graph(e));
+            LBM_TRY(echeck(e, cudaGraphLaunch(e->graph, e->stream), "graph launch"));
+            left -= e->graph_steps;   // an even count: the parity is back to 0
+        } else {
+            LBM_TRY(ens_launch(e, e->cur));
+            e->cur ^= 1;
+            left -= 1;
+        }
+    }
+    for (lbm_ctx* c : e->m) {
+        c->cur = e->cur;
+        c->it += n;
+        c->launches += 2LL * n;
+    }
+    LBM_TRY(echeck(e, cudaEventRecord(e->ev[1], e->stream), "ensemble order"));
+    return echeck(e, cudaStreamWaitEvent(ms, e->ev[1], 0), "ensemble order");
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t nmembers) {
+    if (!out || !members || nmembers < 1) return LBM_ERR_ARG;
+    *out = nullptr;
+    lbm_ensemble* e = new lbm_ensemble();
+    e->nl = members[0].nl;
+    e->storage = members[0].storage;
+    int rc = LBM_OK;
+    for (int k = 0; k < nmembers && rc == LBM_OK; ++k) {
+        const lbm_params& p = members[k];
+        if (p.nl != e->nl || p.storage != e->storage) {
+            rc = efail(e, LBM_ERR_ARG, "member %d: every member needs the same lattice and storage", k);
+            break;
+        }
+        if (!(p.ibnd == 1 && p.jbnd == 0 && (p.kbnd == 11 || p.kbnd == 12 || p.kbnd == 21 || p.kbnd == 22))) {
+            rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: the ensemble runs inflow/outflow i, periodic j, closed k", k);
+            break;
+        }
+        if (p.ihrr != 1 || p.nx % 2 != 0 || p.nx < 4) {
+            rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: the ensemble needs ihrr = 1 and an even nx >= 4", k);
+            break;
+        }
+        lbm_ctx* c = nullptr;
+        rc = lbm_create(&c, &p);
+        if (rc != LBM_OK) {
+            efail(e, rc, "member %d: lbm_create failed (%d)", k, rc);
+            break;
+        }
+        e->m.push_back(c);
+        if (!c->idx32) rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: grid too large for the ensemble kernels", k);
+    }
+    const size_t nm = e->m.size();
+    if (rc == LBM_OK) rc = echeck(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int q = 0; q < 2 && rc == LBM_OK; ++q)
+        rc = echeck(e, cudaEventCreateWithFlags(&e->ev[q], cudaEventDisableTiming), "cudaEventCreate");
+    if (rc == LBM_OK) {
+        e->h_mem.resize(nm);
+        std::vector<int> pre((LBM_ENS_VARIANTS + 1) * (nm + 1), 0);
+        for (int v = 0; v <= LBM_ENS_VARIANTS; ++v) {
+            int* P = pre.data() + (size_t)v * (nm + 1);
+            long long tot = 0;
+            for (size_t k = 0; k < nm; ++k) {
+                const SoaGrid& g = e->m[k]->sg;
+                P[k] = (int)tot;
+                if (v < LBM_ENS_VARIANTS) {
+                    const long long pairs = (long long)(g.nx / 2) * g.ny * g.nz;
+                    tot += (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
+                } else {
+                    // k_bc_fold's grid: k-face blocks, then x-ghost blocks
+                    tot += 2LL * g.ny * ((g.nx + 127) / 128) + ((long long)e->nl * g.ny * g.nz + 127) / 128;
+                }
+            }
+            if (tot >= (1LL << 31)) rc = efail(e, LBM_ERR_UNSUPPORTED, "ensemble too large for one launch");
+            P[nm] = (int)tot;
+            e->nblk[v] = (int)tot;
+        }
+        if (rc == LBM_OK) rc = echeck(e, cudaMalloc(&e->d_mem, nm * sizeof(EnsMember)), "cudaMalloc(ensemble)");
+        if (rc == LBM_OK) rc = echeck(e, cudaMalloc(&e->d_prefix, pre.size() * sizeof(int)), "cudaMalloc(ensemble)");
+        if (rc == LBM_OK)
+            rc = echeck(e, cudaMemcpy(e->d_prefix, pre.data(), pre.size() * sizeof(int), cudaMemcpyHostToDevice),
+                        "ensemble layout");
+    }
+    if (rc != LBM_OK) {
+        g_create_err = e->err.empty() ? "lbm_ensemble_create failed" : e->err;
+        lbm_ensemble_destroy(e);
+        return rc;
+    }
+    g_create_err.clear();
+    *out = e;
+    return LBM_OK;
+}
+
+int lbm_ensemble_destroy(lbm_ensemble* e) {
+    if (!e) return LBM_ERR_ARG;
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    if (e->graph) cudaGraphExecDestroy(e->graph);
+    for (cudaEvent_t v : e->ev)
+        if (v) cudaEventDestroy(v);
+    if (e->stream) cudaStreamDestroy(e->stream);
+    cudaFree(e->d_mem);
+    cudaFree(e->d_prefix);
+    for (lbm_ctx* c : e->m) lbm_destroy(c);
+    delete e;
+    return LBM_OK;
+}
+
+const char* lbm_ensemble_last_error(const lbm_ensemble* e) {
+    if (e) return e->err.c_str();
+    return g_create_err.empty() ? "null ensemble" : g_create_err.c_str();
+}
+
+int lbm_ensemble_size(const lbm_ensemble* e, int32_t* nmembers) {
+    if (!e || !nmembers) return LBM_ERR_ARG;
+    *nmembers = (int32_t)e->m.size();
+    return LBM_OK;
+}
+
+int lbm_ensemble_member(lbm_ensemble* e, int32_t m, lbm_ctx** ctx) {
+    if (!e || !ctx) return LBM_ERR_ARG;
+    if (m < 0 || m >= (int32_t)e->m.size()) return efail(e, LBM_ERR_ARG, "member %d out of range", m);
+    *ctx = e->m[m];
+    return LBM_OK;
+}
+
+int lbm_ensemble_step(lbm_ensemble* e, int32_t nsteps) {
+    if (!e || nsteps < 0) return LBM_ERR_ARG;
+    if (nsteps == 0) return LBM_OK;
+    int used = 0;
+    LBM_TRY(ens_align(e, &used));
+    return ens_run(e, nsteps - used, true);
+}
+
+int lbm_ensemble_set_variant(lbm_ensemble* e, int32_t variant) {
+    if (!e) return LBM_ERR_ARG;
+    if (variant < 0 || variant >= LBM_ENS_VARIANTS) return efail(e, LBM_ERR_ARG, "variant %d out of range", variant);
+    e->variant = variant;
+    return LBM_OK;
+}
+
+int lbm_ensemble_set_graph(lbm_ensemble* e, int32_t graph_steps) {
+    if (!e) return LBM_ERR_ARG;
+    if (graph_steps < 0 || graph_steps % 2 != 0)
+        return efail(e, LBM_ERR_ARG, "graph_steps must be 0 (no graph) or a positive even count");
+    if (graph_steps != e->graph_steps && e->graph) {
+        cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+    }
+    e->graph_steps = graph_steps;
+    return LBM_OK;
+}
+
+int lbm_ensemble_autotune(lbm_ensemble* e, int32_t trial_steps, int32_t* variant, float* ms_per_step) {
+    if (!e || trial_steps < 1) return LBM_ERR_ARG;
+    int used = 0;
+    LBM_TRY(ens_align(e, &used));
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    LBM_TRY(echeck(e, cudaEventCreate(&t0), "cudaEventCreate"));
+    int rc = echeck(e, cudaEventCreate(&t1), "cudaEventCreate");
+    float best = 0.f;
+    int bestv = e->variant;
+    for (int v = 0; v < LBM_ENS_VARIANTS && rc == LBM_OK; ++v) {
+        e->variant = v;
+        rc = ens_run(e, 1, false);   // warm-up
+        if (rc == LBM_OK) rc = echeck(e, cudaEventRecord(t0, e->stream), "autotune");
+        if (rc == LBM_OK) rc = ens_run(e, trial_steps, false);
+        if (rc == LBM_OK) rc = echeck(e, cudaEventRecord(t1, e->stream), "autotune");
+        if (rc == LBM_OK) rc = echeck(e, cudaEventSynchronize(t1), "autotune");
+        float ms = 0.f;
+        if (rc == LBM_OK) rc = echeck(e, cudaEventElapsedTime(&ms, t0, t1), "autotune");
+        if (rc != LBM_OK) break;
+        ms /= (float)trial_steps;
+        if (ms_per_step) ms_per_step[v] = ms;
+        if (v == 0 || ms < best) {
+            best = ms;
+            bestv = v;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    e->variant = bestv;
+    if (variant) *variant = bestv;
+    return rc;
+}
+
+}  // extern "C"

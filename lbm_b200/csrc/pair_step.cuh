@@ -293,18 +293,10 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
     }
 }
 
-#ifndef LBM_PAIR_MIN_BLOCKS
-#define LBM_PAIR_MIN_BLOCKS 5
-#endif
-// Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
-// ihrr = 1, nx even and Q * dstride < 2^31.
+// One pair (i, i+1), i odd, of row (j, k): pull, collide, store.
 template <int Q, typename S, bool WRAP>
-__global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
-                                                                        StepArgs a) {
-    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
-    const int j = blockIdx.y + 1;
-    const int k = blockIdx.z + 1;
-    if (i > a.g.nx) return;
+__device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restrict__ dst, const StepArgs& a, int i, int j,
+                                          int k) {
     const long long o = a.g.off(i, j, k);
     f2 fp[Q];
     {
@@ -315,6 +307,19 @@ __global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S*
         PairLoad<Q, S, 0>::run(fp, p0, pyp, pym, a);
     }
     pair_update<Q, S, WRAP>(fp, dst, a, o, i, j, k);
+}
+
+#ifndef LBM_PAIR_MIN_BLOCKS
+#define LBM_PAIR_MIN_BLOCKS 5
+#endif
+// Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
+// ihrr = 1, nx even and Q * dstride < 2^31.
+template <int Q, typename S, bool WRAP>
+__global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
+                                                                        StepArgs a) {
+    const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
+    if (i > a.g.nx) return;
+    pair_cell<Q, S, WRAP>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);
 }
 
 }  // namespace lbm

@@ -149,12 +149,14 @@ __device__ __forceinline__ void store_sector(S* p, S v, int slot) {
 //     k-ghost cell that the reference's k-face copies it to (sources i-cx = 0
 //     or nx+1; always a pulled direction, so it is in the rows), so each
 //     x-ghost element is read and then written by one and the same thread.
+// vb: this block's index among the nface_blocks + x-ghost blocks of the grid
+// (blocks of 128 threads).
 template <int Q, typename S>
-__global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
+__device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs& a, int nface_blocks, int vb) {
     const SoaGrid& g = a.g;
-    if ((int)blockIdx.x < nface_blocks) {
+    if (vb < nface_blocks) {
         const int per_row = (g.nx + 127) / 128;
-        const int b = blockIdx.x;
+        const int b = vb;
         const int side = b / (per_row * g.ny);
         const int j = (b / per_row) % g.ny + 1;
         const int i = (b % per_row) * 128 + threadIdx.x + 1;
@@ -175,7 +177,7 @@ __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a,
         return;
     }
     // x-ghost threads
-    const long long e = (long long)(blockIdx.x - nface_blocks) * blockDim.x + threadIdx.x;
+    const long long e = (long long)(vb - nface_blocks) * 128 + threadIdx.x;
     const long long nyz = (long long)g.ny * g.nz;
     if (e >= (long long)Q * nyz) return;
     if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
@@ -221,6 +223,11 @@ __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a,
         if (a.full_sector) store_sector<S>(p, gout, 0);
         else *p = gout;
     }
+}
+
+template <int Q, typename S>
+__global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
+    bc_fold_block<Q, S>(f1, f2, a, nface_blocks, blockIdx.x);
 }
 
 // Folded configuration: copy the x-ghost columns of a buffer whose rows hold

@@ -59,6 +59,23 @@ CHANNEL_Q19_SMALL = CHANNEL_Q27_SMALL.with_(name="turb_inflow_q19_256x128x128", 
 CITY_Q27 = CHANNEL_Q27.with_(name="city_q27_512x256x256", city=16)
 CITY_Q27_REDUCED = CITY_Q27.with_(name="city_q27_128x64x64", nx=128, ny=64, nz=64)
 
+def ensemble_members(n: int = 64, seed: int = 0, nl: int = 19, storage_steps: int = 500) -> list:
+    """Members of the batched-ensemble workload: sizes drawn from the seed with
+    nx in [96, 192] and ny, nz in [48, 96], each a multiple of 8; each member has
+    its own inflow speed, uniform in [0.03, 0.07], and its own inflow-turbulence
+    seed (amplitude 1e-4 at i = 10); physics as the sphere case without solids."""
+    rng = np.random.default_rng(seed + 31337)
+    out = []
+    for m in range(n):
+        nx = 8 * int(rng.integers(12, 25))
+        ny = 8 * int(rng.integers(6, 13))
+        nz = 8 * int(rng.integers(6, 13))
+        uin = float(rng.uniform(0.03, 0.07))
+        out.append(Workload("ensemble_member_%02d" % m, nx, ny, nz, nl, steps=storage_steps, uin=uin, lturb=True,
+                            ampl=1.0e-4, seed=1000 * seed + m + 1))
+    return out
+
+
 WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL,
                                  CITY_Q27, CITY_Q27_REDUCED)}
 

@@ -41,7 +41,7 @@ def test_library_exports_every_header_symbol(lib):
 
 
 def test_bindings_cover_header():
-    bound = set(_lib.SIGNATURES) | {"lbm_last_error"}
+    bound = set(_lib.SIGNATURES) | {"lbm_last_error", "lbm_ensemble_last_error"}
     assert set(header_functions()) == bound
 
 
