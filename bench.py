@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--no-f16", action="store_true", help="skip the FP16-offset storage comparison")
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
+    ap.add_argument("--adjoint", action="store_true",
+                    help="checkpointed adjoint sweep of a probe-misfit loss (D3Q19 256x128x128 sphere, 100 steps)")
     ap.add_argument("--accuracy", action="store_true",
                     help="FP16-offset storage error study (city workload) instead of the timing run")
     return ap.parse_args()
@@ -483,8 +485,83 @@ def ensemble_bench(a):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# adjoint: probe-misfit gradient through 100 steps, checkpoints every 10
+# ---------------------------------------------------------------------------
+def adjoint_bench(a):
+    """Time of the checkpointed reverse sweep against the forward run it
+    differentiates (the per-call path, keeping checkpoints), and against the
+    fused forward step for the same steps."""
+    import torch
+    from lbm_b200 import Params, Solver, workloads as W
+    from lbm_b200.adjoint import ProbeProblem, initial_state
+    torch.cuda.set_device(0)
+    wl = W.ADJOINT_Q19
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=10,
+               kinevisc=wl.kinevisc)
+    blank = torch.from_numpy(W.blanking(wl)).cuda()
+    probes = W.probe_cells(wl, 200, 0)
+    pb = ProbeProblem(p, probes, wl.steps, blanking=blank, checkpoint=10)
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(wl))
+    uvel = torch.from_numpy(W.inflow_profile(wl)).cuda()
+    f1, f2 = initial_state(pb.lbm, rho, u, v, w, uvel)
+    R = pb._macro(f1)
+    for _ in range(20):                       # leave the exact initial equilibrium
+        f1, f2 = pb._step(f1, f2, R, uvel)
+    truth = pb.forward(f1, f2, uvel + torch.from_numpy(W.inflow_perturbation(wl.nz, 0, 5e-3)).cuda(), keep=False)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+    pb.forward(f1, f2, uvel)                  # warm-up of every kernel
+    pb.backward(torch.zeros(len(probes), 3, device="cuda"))
+    torch.cuda.synchronize()
+    e0, e1, e2 = ev(), ev(), ev()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record()
+        up = pb.forward(f1, f2, uvel)
+        e1.record()
+        gf, gu = pb.backward(2.0 * (up - truth))
+        e2.record()
+        torch.cuda.synchronize()
+    t_fwd, t_bwd = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    loss = float(((up.double() - truth.double()) ** 2).sum())
+    gnorm_f, gnorm_u = float(gf.double().norm()), float(gu.double().norm())
+    pb.close()
+    torch.cuda.empty_cache()
+    # the fused forward for the same steps, for scale
+    s = Solver(p, rho, u, v, w, uvel, blanking=blank)
+    s.step(3)
+    torch.cuda.synchronize()
+    f0, f9 = ev(), ev()
+    f0.record()
+    s.step(wl.steps)
+    f9.record()
+    torch.cuda.synchronize()
+    t_fused = f0.elapsed_time(f9)
+    s.close()
+    cells = wl.cells
+    line = {"metric": "adjoint sweep time over forward time (probe-misfit gradient, checkpoint-and-recompute)",
+            "value": round(t_bwd / t_fwd, 3), "unit": "x forward (per-call path)", "n_gpus": 1, "steps": wl.steps,
+            "warmup": 1, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded initial field, probes and inflow perturbation)",
+            "config": {"workload": wl.name, "grid": [wl.nx, wl.ny, wl.nz], "lattice": "D3Q19",
+                       "sphere": list(wl.sphere), "probes": len(probes), "checkpoint_every": 10,
+                       "controls": "initial f1 (rho, u recomputed from it) and the inflow profile uvel(k)",
+                       "target": "same run with uvel + 5e-3 smooth seeded noise"},
+            "forward_ms": round(t_fwd, 2), "reverse_ms": round(t_bwd, 2),
+            "fused_forward_ms": round(t_fused, 2), "reverse_over_fused_forward": round(t_bwd / t_fused, 3),
+            "forward_mlups": round(cells * wl.steps / (t_fwd * 1e-3) / 1e6, 1),
+            "loss": loss, "grad_norm": {"f1": gnorm_f, "uvel": gnorm_u},
+            "gradient_check": "tests/test_gpu_adjoint.py: central FP64 differences, 8 seeded directions, rel <= 1e-4",
+            "clocks": clk.report()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.adjoint and a.impl == "ours":
+        return adjoint_bench(a)
     if a.ensemble and a.impl == "ours":
         return ensemble_bench(a)
     from lbm_b200 import workloads as W

@@ -196,6 +196,41 @@ int lbm_conservation(lbm_ctx* ctx, double* out_host);
 int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
                               void* stream);
 
+/* ---- adjoint (reverse-mode) kernels of the per-call path ----
+ * No counterpart in the reference, which has no gradients.  Each entry point
+ * takes the adjoint (gradient of a scalar loss) of a forward call's outputs and
+ * returns the adjoint of its inputs, evaluated at the forward inputs passed in;
+ * chaining them in the reverse of main.F90's step order (macrovars, drift,
+ * boundarycond, solids, postcoll) back-propagates through time steps.  Arrays
+ * are device arrays in the reference layout, like the forward calls.  The
+ * adjoint of lbm_solids is lbm_solids itself (a swap of opposite directions). */
+/* postcoll: fhat holds the adjoint of postcoll's output f on entry and the adjoint
+ * of its input f on exit (interior cells; ghost cells untouched); rhohat..what
+ * are incremented by the adjoints of rho, u, v, w.  f, tau, rho..w, ablvisc: the
+ * forward inputs (tau is read only when ivreman = 0 and may be NULL otherwise;
+ * ablvisc may be NULL).  blanking (may be NULL): the adjoint of a lbm_solids call
+ * that followed postcoll is applied first.  Regularized collision (ihrr = 1) only. */
+int lbm_postcoll_adj(lbm_ctx* ctx, float* fhat, const float* f, const float* tau, const float* rho, const float* u,
+                     const float* v, const float* w, const float* ablvisc, float* rhohat, float* uhat, float* vhat,
+                     float* what, const int32_t* blanking);
+/* macrovars: fhat += (d rho,u,v,w / d f)^T (rhohat, uhat, vhat, what) at the forward input f, all cells */
+int lbm_macrovars_adj(lbm_ctx* ctx, float* fhat, const float* rhohat, const float* uhat, const float* vhat,
+                      const float* what, const float* f);
+/* drift(f_out, f_in): fhat_in += pull^T fhat_out, then the interior of fhat_out is
+ * zeroed (drift overwrote it); the ghost cells of fhat_out stay (they belong to
+ * the older values drift left in place) */
+int lbm_drift_adj(lbm_ctx* ctx, float* fhat_in, float* fhat_out);
+/* lbm_macrovars_adj on the drift's output followed by lbm_drift_adj, in one pass:
+ * the macrovars adjoints (at interior cells) enter through the forward outputs
+ * rho, u, v, w of that macrovars call, so the drift's output f is not read */
+int lbm_macrovars_drift_adj(lbm_ctx* ctx, float* fhat_in, float* fhat_out, const float* rhohat, const float* uhat,
+                            const float* vhat, const float* what, const float* rho, const float* u, const float* v,
+                            const float* w);
+/* boundarycond(f1, f2, uvel): the adjoint of every ghost value it wrote in f1 is
+ * passed to its sources in f1hat / f2hat and, for the inflow ghosts, to uvelhat
+ * (incremented; needed when ibnd = 1), then zeroed */
+int lbm_boundarycond_adj(lbm_ctx* ctx, float* f1hat, float* f2hat, float* uvelhat);
+
 /* ---- batched ensemble ----
  * No counterpart in the reference, which runs one domain per process (main.F90).
  * An ensemble holds many independent members of different sizes, each an

@@ -85,6 +85,11 @@ SIGNATURES = {
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],
+    "lbm_postcoll_adj": [P, P, P, P, P, P, P, P, P, P, P, P, P, P],
+    "lbm_macrovars_adj": [P, P, P, P, P, P, P],
+    "lbm_drift_adj": [P, P, P],
+    "lbm_macrovars_drift_adj": [P, P, P, P, P, P, P, P, P, P, P],
+    "lbm_boundarycond_adj": [P, P, P, P],
     "lbm_ensemble_create": [ctypes.POINTER(P), ctypes.POINTER(LbmParams), I],
     "lbm_ensemble_destroy": [P],
     "lbm_ensemble_size": [P, ctypes.POINTER(ctypes.c_int32)],

@@ -1,0 +1,132 @@
+"""Gradients of a probe-misfit loss through N time steps of the per-call path.
+
+The forward run is main.F90's loop (main.F90:283-329, without the inflow
+turbulence): per step postcoll, solids, boundarycond, drift, swap, macrovars,
+on the library's per-call kernels.  The state of step n is (f1, f2, rho/u/v/w),
+with rho, u, v, w = macrovars(f1); the controls are the initial f1 (its rho, u,
+v, w recomputed from it) and the inflow profile uvel(k) that boundarycond uses
+in every step.
+
+The reverse sweep chains the library's adjoint kernels in the opposite order
+(macrovars and drift in one pass, boundarycond, then solids and postcoll in
+one pass).  Memory is bounded by
+checkpoint-and-recompute: the forward keeps (f1, f2) every ``checkpoint``
+steps; the reverse sweep replays each segment from its checkpoint, keeping the
+segment's states, and walks back through it.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .api import Lbm, Params
+
+
+class ProbeProblem:
+    """u at probe cells after ``nsteps`` steps, and the reverse sweep of its loss.
+
+    probes: int array (P, 3) of 1-based interior (i, j, k) cells."""
+
+    def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
+        self.p = params
+        self.lbm = Lbm(params)
+        self.nsteps = int(nsteps)
+        self.K = max(1, int(checkpoint))
+        self.blanking = blanking
+        pr = np.asarray(probes, dtype=np.int64)
+        self.probes = pr
+        # flat indices into the (nz+2, ny+2, nx+2) scalar fields
+        self.pidx = torch.from_numpy((pr[:, 2] * (params.ny + 2) + pr[:, 1]) * (params.nx + 2) + pr[:, 0]).cuda()
+        self.tau = torch.full(params.sshape, 3.0 * params.kinevisc + 0.5, dtype=torch.float32, device="cuda")
+        self.ckpt = {}
+
+    # ---- forward ----------------------------------------------------------------------
+    def _macro(self, f):
+        L = self.lbm
+        R = [L.empty_s() for _ in range(4)]
+        L.macrovars(*R, f)
+        return R
+
+    def _step(self, A, B, R, uvel):
+        """one step in place of main.F90's order; returns the new (f1, f2)"""
+        L = self.lbm
+        L.postcoll(A, self.tau, *R)
+        if self.blanking is not None:
+            L.solids(A, self.blanking)
+        L.boundarycond(A, B, uvel)
+        L.drift(B, A)
+        A, B = B, A
+        L.macrovars(*R, A)
+        return A, B
+
+    def probe_u(self, R):
+        return torch.stack([R[q].reshape(-1)[self.pidx] for q in (1, 2, 3)], dim=1)
+
+    def forward(self, f1, f2, uvel, keep: bool = True):
+        """u, v, w at the probes after nsteps; keeps the checkpoints for backward()."""
+        A, B = f1.clone(), f2.clone()
+        R = self._macro(A)
+        self.ckpt = {}
+        self.uvel = uvel.contiguous()
+        for n in range(self.nsteps):
+            if keep and n % self.K == 0:
+                self.ckpt[n] = (A.clone(), B.clone())
+            A, B = self._step(A, B, R, self.uvel)
+        return self.probe_u(R)
+
+    # ---- reverse ----------------------------------------------------------------------
+    def backward(self, uhat_probes):
+        """Adjoint of the probe velocities (P, 3) -> (d loss / d f1 initial, d loss / d uvel)."""
+        L = self.lbm
+        Ah, Bh = L.empty_f(), L.empty_f()
+        Rh = [L.empty_s() for _ in range(4)]
+        for q in range(3):
+            Rh[q + 1].view(-1).index_add_(0, self.pidx, uhat_probes[:, q].contiguous().float())
+        uvel_h = torch.zeros(self.p.nz, dtype=torch.float32, device="cuda")
+        starts = sorted(self.ckpt)
+        for s in reversed(starts):
+            e = min(s + self.K, self.nsteps)
+            A, B = (t.clone() for t in self.ckpt[s])
+            R = self._macro(A)
+            states = []                       # (A_n, R_n) of the segment
+            for n in range(s, e):
+                states.append((A.clone(), [t.clone() for t in R]))
+                A, B = self._step(A, B, R, self.uvel)
+            R_next = R
+            for n in range(e - 1, s - 1, -1):
+                A_n, R_n = states[n - s]
+                Ah, Bh, Rh = self._reverse_step(Ah, Bh, Rh, A_n, R_n, R_next, uvel_h)
+                R_next = R_n
+            del states
+        A0 = self.ckpt[0][0]
+        L.macrovars_adj(Ah, *Rh, A0)          # rho, u, v, w of step 0 are macrovars(f1)
+        return Ah, uvel_h
+
+    def _reverse_step(self, Ah, Bh, Rh, A_n, R_n, R_next, uvel_h):
+        L = self.lbm
+        W = Bh                                # f2 of step n+1 is the post-collision f1 of step n
+        # macrovars(f1(n+1)) then drift: interior of f1(n+1) = pull(post-collision f1)
+        L.macrovars_drift_adj(W, Ah, *Rh, *R_next)
+        for t in Rh:
+            t.zero_()
+        Bn = Ah                               # f1(n+1)'s ghost cells are f2(n)'s
+        L.boundarycond_adj(W, Bn, uvel_h)
+        # solids (a swap, its own adjoint) folded into the postcoll adjoint
+        L.postcoll_adj(W, A_n, *R_n, *Rh, tau=self.tau, blanking=self.blanking)
+        return W, Bn, Rh
+
+    def close(self):
+        self.ckpt = {}
+        self.lbm.close()
+
+
+def initial_state(lbm: Lbm, rho, u, v, w, uvel):
+    """(f1, f2) as main.F90:243-247 initialises them: fequil3, fillghosts, f1 = f2,
+    boundarycond twice."""
+    fB = lbm.empty_f()
+    lbm.fequil3(fB, rho, u, v, w)
+    lbm.fillghosts(fB)
+    fA = fB.clone()
+    lbm.boundarycond(fB, fA, uvel)
+    lbm.boundarycond(fA, fB, uvel)
+    return fA, fB

@@ -196,6 +196,37 @@ class Lbm:
         self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
         self._call("lbm_inflow_turbulence_apply", _ptr(f), _ptr(df))
 
+    # ---- adjoints of the per-call kernels (reverse mode) -------------------------------
+    def postcoll_adj(self, fhat, f, rho, u, v, w, rhohat, uhat, vhat, what, tau=None, ablvisc=None, blanking=None):
+        """fhat: adjoint of postcoll's output f in, of its input f out; rhohat..what incremented.
+        blanking: apply the adjoint of a following solids call first."""
+        self._f(fhat, f)
+        self._s(rho, u, v, w, rhohat, uhat, vhat, what, tau)
+        self._chk(blanking, self.p.sshape, dtype=torch.int32, name="blanking")
+        self._call("lbm_postcoll_adj", _ptr(fhat), _ptr(f), _ptr(tau), _ptr(rho), _ptr(u), _ptr(v), _ptr(w),
+                   _ptr(ablvisc), _ptr(rhohat), _ptr(uhat), _ptr(vhat), _ptr(what), _ptr(blanking))
+
+    def macrovars_drift_adj(self, fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w):
+        """macrovars_adj (on the drift output, interior cells) then drift_adj, in one pass."""
+        self._f(fhat_in, fhat_out)
+        self._s(rhohat, uhat, vhat, what, rho, u, v, w)
+        self._call("lbm_macrovars_drift_adj", _ptr(fhat_in), _ptr(fhat_out), _ptr(rhohat), _ptr(uhat), _ptr(vhat),
+                   _ptr(what), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+
+    def macrovars_adj(self, fhat, rhohat, uhat, vhat, what, f):
+        self._f(fhat, f)
+        self._s(rhohat, uhat, vhat, what)
+        self._call("lbm_macrovars_adj", _ptr(fhat), _ptr(rhohat), _ptr(uhat), _ptr(vhat), _ptr(what), _ptr(f))
+
+    def drift_adj(self, fhat_in, fhat_out):
+        self._f(fhat_in, fhat_out)
+        self._call("lbm_drift_adj", _ptr(fhat_in), _ptr(fhat_out))
+
+    def boundarycond_adj(self, f1hat, f2hat, uvelhat):
+        self._f(f1hat, f2hat)
+        self._chk(uvelhat, (self.p.nz,), name="uvelhat")
+        self._call("lbm_boundarycond_adj", _ptr(f1hat), _ptr(f2hat), _ptr(uvelhat))
+
     def fillghosts(self, f):
         self._f(f)
         self._call("lbm_fillghosts", _ptr(f))

@@ -1,0 +1,381 @@
+// adjoint.cuh -- reverse-mode (vector-Jacobian) kernels of the per-call path,
+// in the reference layout f(nl,0:nx+1,0:ny+1,0:nz+1).
+//
+// Each kernel takes the adjoint of a forward kernel's outputs and returns the
+// adjoint of its inputs, at the forward inputs it is given (the forward values
+// are recomputed where needed, never stored):
+//   postcoll   (m_postcoll_kernel.F90:70-245, regularized, optional Vreman)
+//   macrovars  (m_macrovars_kernel.F90:35-49)
+//   drift      (m_drift_kernel.F90:37-42): the transpose of the pull is a push
+// The adjoint of solids (a swap of opposite directions) is solids itself, and
+// the adjoint of boundarycond runs the boundary kernels of boundary.cuh in
+// reverse order with the AdjAcc accessor below.  Derivatives are exact for the
+// arithmetic of the forward kernels (collide.cuh), taken by hand.
+#pragma once
+
+#include "collide.cuh"
+#include "ref_kernels.cuh"
+
+namespace lbm {
+
+// Reverse of one regularized collision (ihrr = 1, no turbulence slice, no solid
+// flag: postcoll has none).  fp: the cell's pre-collision offsets f - w;
+// gh: adjoint of the post-collision populations.  fh receives the adjoint of
+// the pre-collision populations; rh, uxh, uyh, uzh are incremented by the
+// adjoint of postcoll's rho, u, v, w inputs.
+template <int Q>
+__device__ __forceinline__ void collide_adj(const float (&fp)[Q], const float (&gh)[Q], float rho, float ux, float uy,
+                                            float uz, const CollideParams& cp, float abl, float tau_in, float (&fh)[Q],
+                                            float& rh, float& uxh, float& uyh, float& uzh) {
+    // ---- forward values (as collide()) ----
+    const Moments m = moments<Q>(fp);
+    const float third = 1.0f / 3.0f;
+    const float rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const float axx = m.pxx - m.s0 * third - rux * ux;
+    const float ayy = m.pyy - m.s0 * third - ruy * uy;
+    const float azz = m.pzz - m.s0 * third - ruz * uz;
+    const float axy = m.pxy - rux * uy;
+    const float axz = m.pxz - rux * uz;
+    const float ayz = m.pyz - ruy * uz;
+    const float tr = axx + ayy + azz;
+    float tau = tau_in;
+    float amag0 = 0.f, amag = 0.f, b11 = 0.f, b22 = 0.f, b33 = 0.f, b12 = 0.f, b13 = 0.f, b23 = 0.f, bb = 0.f, t = 0.f;
+    if (cp.ivreman) {
+        amag0 = axx * axx + ayy * ayy + azz * azz + 2.0f * (axy * axy + axz * axz + ayz * ayz);
+        amag = fmaxf(amag0, 1.17549435e-38f);
+        b11 = cp.eps + axx * axx + axy * axy + axz * axz;
+        b22 = cp.eps + axy * axy + ayy * ayy + ayz * ayz;
+        b33 = cp.eps + axz * axz + ayz * ayz + azz * azz;
+        b12 = cp.eps + axx * axy + axy * ayy + axz * ayz;
+        b13 = cp.eps + axx * axz + axy * ayz + axz * azz;
+        b23 = cp.eps + axy * axz + ayy * ayz + ayz * azz;
+        bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+        t = bb / amag;
+        const float nut = (t > cp.eps) ? cp.cvre * sqrtf(t) : 0.0f;
+        tau = 3.0f * (cp.kinevisc + nut + abl) + 0.5f;
+    }
+    const float K = 1.0f - 1.0f / tau;
+    const bool cubic = (cp.ibgk == 3);
+    const float usq = ux * ux + uy * uy + uz * uz;
+    const float R45 = 4.5f * rho;
+    const float R45o = cubic ? R45 : 0.0f;
+    const float B0 = 3.0f * rho - (cubic ? R45 * usq : 0.0f);
+    const float D0 = B0 - 4.5f * K * tr;
+    const float K45 = 4.5f * K, K135 = 13.5f * K, K9 = 9.0f * K;
+    const float vx = axx * ux + axy * uy + axz * uz;
+    const float vy = axy * ux + ayy * uy + ayz * uz;
+    const float vz = axz * ux + ayz * uy + azz * uz;
+
+    // ---- reverse (C0 = A0 - 1.5 K tr with A0 = (rho - 1) - 1.5 rho |u|^2 enter only through their adjoints) ----
+    float C0h = lat_w<Q>(0) * gh[0];
+    float R45h = 0.f, R45oh = 0.f, K45h = 0.f, K135h = 0.f, K9h = 0.f, D0h = 0.f;
+    float axxh = 0.f, ayyh = 0.f, azzh = 0.f, axyh = 0.f, axzh = 0.f, ayzh = 0.f;
+    float vxh = 0.f, vyh = 0.f, vzh = 0.f;
+#pragma unroll
+    for (int l = 1; l < Q; l += 2) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        const float w = lat_w<Q>(l);
+        const float cu = cdot(cx, cy, cz, ux, uy, uz);
+        float cac = 0.f;
+        macc(cac, cx * cx, axx);
+        macc(cac, cy * cy, ayy);
+        macc(cac, cz * cz, azz);
+        macc(cac, cx * cy, 2.0f * axy);   // macc takes coefficients -1, 0, 1
+        macc(cac, cx * cz, 2.0f * axz);
+        macc(cac, cy * cz, 2.0f * ayz);
+        const float cau = cdot(cx, cy, cz, vx, vy, vz);
+        const float cu2 = cu * cu;
+        const float Eh = w * (gh[l] + gh[l + 1]);   // f(l) = E + O, f(opposite) = E - O
+        const float Oh = w * (gh[l] - gh[l + 1]);
+        const float inner = D0 + R45o * cu2 + K135 * cac;
+        // E / w = C0 + R45 cu^2 + K45 cac
+        C0h += Eh;
+        R45h += Eh * cu2;
+        K45h += Eh * cac;
+        float cuh = Eh * R45 * 2.0f * cu;
+        float cach = Eh * K45;
+        // O / w = cu (D0 + R45o cu^2 + K135 cac) - K9 cau
+        cuh += Oh * (inner + 2.0f * R45o * cu2);
+        D0h += Oh * cu;
+        R45oh += Oh * cu * cu2;
+        K135h += Oh * cu * cac;
+        cach += Oh * cu * K135;
+        K9h -= Oh * cau;
+        const float cauh = -Oh * K9;
+        macc(uxh, cx, cuh);
+        macc(uyh, cy, cuh);
+        macc(uzh, cz, cuh);
+        macc(axxh, cx * cx, cach);
+        macc(ayyh, cy * cy, cach);
+        macc(azzh, cz * cz, cach);
+        macc(axyh, cx * cy, 2.0f * cach);
+        macc(axzh, cx * cz, 2.0f * cach);
+        macc(ayzh, cy * cz, 2.0f * cach);
+        macc(vxh, cx, cauh);
+        macc(vyh, cy, cauh);
+        macc(vzh, cz, cauh);
+    }
+    // v = a u
+    axxh += vxh * ux;
+    ayyh += vyh * uy;
+    azzh += vzh * uz;
+    axyh += vxh * uy + vyh * ux;
+    axzh += vxh * uz + vzh * ux;
+    ayzh += vyh * uz + vzh * uy;
+    uxh += vxh * axx + vyh * axy + vzh * axz;
+    uyh += vxh * axy + vyh * ayy + vzh * ayz;
+    uzh += vxh * axz + vyh * ayz + vzh * azz;
+    // K45, K135, K9; C0 = A0 - 1.5 K tr; D0 = B0 - 4.5 K tr
+    float Kh = 4.5f * K45h + 13.5f * K135h + 9.0f * K9h - 1.5f * tr * C0h - 4.5f * tr * D0h;
+    const float trh = -1.5f * K * C0h - 4.5f * K * D0h;
+    const float A0h = C0h, B0h = D0h;
+    if (cubic) R45h += R45oh;
+    float usqh = 0.f;
+    rh += 3.0f * B0h;
+    if (cubic) {
+        R45h -= usq * B0h;
+        usqh -= R45 * B0h;
+    }
+    rh += A0h * (1.0f - 1.5f * usq);
+    usqh -= 1.5f * rho * A0h;
+    rh += 4.5f * R45h;
+    uxh += 2.0f * ux * usqh;
+    uyh += 2.0f * uy * usqh;
+    uzh += 2.0f * uz * usqh;
+    axxh += trh;
+    ayyh += trh;
+    azzh += trh;
+    // K = 1 - 1/tau, tau = 3 (nu + nut + abl) + 1/2, nut = cvre sqrt(bb / amag) where bb / amag > eps
+    if (cp.ivreman && t > cp.eps) {
+        const float nuth = 3.0f * Kh / (tau * tau);
+        const float th = nuth * cp.cvre * 0.5f / sqrtf(t);
+        const float bbh = th / amag;
+        const float amagh = (amag0 >= 1.17549435e-38f) ? -th * bb / (amag * amag) : 0.0f;
+        const float b11h = bbh * (b22 + b33), b22h = bbh * (b11 + b33), b33h = bbh * (b11 + b22);
+        const float b12h = -2.0f * b12 * bbh, b13h = -2.0f * b13 * bbh, b23h = -2.0f * b23 * bbh;
+        axxh += 2.0f * axx * b11h + axy * b12h + axz * b13h + 2.0f * axx * amagh;
+        ayyh += 2.0f * ayy * b22h + axy * b12h + ayz * b23h + 2.0f * ayy * amagh;
+        azzh += 2.0f * azz * b33h + axz * b13h + ayz * b23h + 2.0f * azz * amagh;
+        axyh += 2.0f * axy * (b11h + b22h) + (axx + ayy) * b12h + ayz * b13h + axz * b23h + 4.0f * axy * amagh;
+        axzh += 2.0f * axz * (b11h + b33h) + ayz * b12h + (axx + azz) * b13h + axy * b23h + 4.0f * axz * amagh;
+        ayzh += 2.0f * ayz * (b22h + b33h) + axz * b12h + axy * b13h + (ayy + azz) * b23h + 4.0f * ayz * amagh;
+    }
+    // a_ij = p_ij - s0/3 delta_ij - rho u_i u_j
+    const float s0h = -(axxh + ayyh + azzh) * third;
+    rh -= axxh * ux * ux + ayyh * uy * uy + azzh * uz * uz + axyh * ux * uy + axzh * ux * uz + ayzh * uy * uz;
+    uxh -= rho * (2.0f * ux * axxh + uy * axyh + uz * axzh);
+    uyh -= rho * (2.0f * uy * ayyh + ux * axyh + uz * ayzh);
+    uzh -= rho * (2.0f * uz * azzh + ux * axzh + uy * ayzh);
+    // moments are linear in f
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        float v = s0h;
+        macc(v, cx * cx, axxh);
+        macc(v, cy * cy, ayyh);
+        macc(v, cz * cz, azzh);
+        macc(v, cx * cy, axyh);
+        macc(v, cx * cz, axzh);
+        macc(v, cy * cz, ayzh);
+        fh[l] = v;
+    }
+}
+
+// postcoll adjoint over interior cells: fh holds the adjoint of postcoll's output
+// f on entry and the adjoint of its input f on exit (ghost cells untouched);
+// rhoh, uh, vh, wh are incremented.  f, rho, u, v, w, tau, abl: postcoll's inputs.
+// blank (may be null): the adjoint of a solids call that followed postcoll is
+// applied first (a swap of opposite directions at blanked cells).
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_postcoll_adj(float* fh, const float* f, const float* rho, const float* u,
+                                                          const float* v, const float* w, const float* tau,
+                                                          const float* abl, float* rhoh, float* uh, float* vh,
+                                                          float* wh, const int32_t* blank, RefGrid g, CollideParams cp) {
+    __shared__ float sf[128 * Q];
+    __shared__ float sg[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sf, f, g.cell(i0, j, k), n);
+    tile_load<Q>(sg, fh, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        float fp[Q], gh[Q], out[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            fp[l] = sf[t * Q + l] - lat_w<Q>(l);
+            gh[l] = sg[t * Q + l];
+        }
+        if (blank && blank[c] != 0) {
+#pragma unroll
+            for (int l = 1; l + 1 < Q; l += 2) {
+                const float x = gh[l];
+                gh[l] = gh[l + 1];
+                gh[l + 1] = x;
+            }
+        }
+        float rr = 0.f, ux = 0.f, uy = 0.f, uz = 0.f;
+        collide_adj<Q>(fp, gh, rho[c], u[c], v[c], w[c], cp, abl ? abl[k - 1] : 0.0f, tau[c], out, rr, ux, uy, uz);
+        rhoh[c] += rr;
+        uh[c] += ux;
+        vh[c] += uy;
+        wh[c] += uz;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) sg[t * Q + l] = out[l];
+    }
+    __syncthreads();
+    tile_store<Q>(sg, fh, g.cell(i0, j, k), n);
+}
+
+// macrovars adjoint over the ghost-inclusive grid: fh += d(rho, u, v, w)/df^T (rhoh, uh, vh, wh)
+// with rho = sum f, u = (sum c f) / rho at the forward input f.
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_macrovars_adj(float* fh, const float* rhoh, const float* uh,
+                                                           const float* vh, const float* wh, const float* f,
+                                                           RefGrid g) {
+    __shared__ float sf[128 * Q];
+    __shared__ float sg[128 * Q];
+    const int i0 = blockIdx.x * 128, j = blockIdx.y, k = blockIdx.z;
+    const int n = min(128, g.nx + 2 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sf, f, g.cell(i0, j, k), n);
+    tile_load<Q>(sg, fh, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        float tr = 0.f, tu = 0.f, tv = 0.f, tw = 0.f;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            const float tf = sf[t * Q + l];
+            tr += tf;
+            macc(tu, lat_cx(l), tf);
+            macc(tv, lat_cy(l), tf);
+            macc(tw, lat_cz(l), tf);
+        }
+        const float inv = 1.0f / tr;
+        const float ux = tu * inv, uy = tv * inv, uz = tw * inv;
+        const float ax = uh[c] * inv, ay = vh[c] * inv, az = wh[c] * inv;
+        const float base = rhoh[c] - (ax * ux + ay * uy + az * uz);
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            float d = base;
+            macc(d, lat_cx(l), ax);
+            macc(d, lat_cy(l), ay);
+            macc(d, lat_cz(l), az);
+            sg[t * Q + l] += d;
+        }
+    }
+    __syncthreads();
+    tile_store<Q>(sg, fh, g.cell(i0, j, k), n);
+}
+
+// drift adjoint, gather form: fh_in(l, y) += fh_out(l, y + c_l) where y + c_l is
+// an interior cell.  A thread per (l, i) of a row y over the ghost-inclusive grid.
+__global__ void k_ref_drift_adj(float* fh_in, const float* fh_out, RefGrid g) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int nl = g.nl;
+    if (idx >= nl * (g.nx + 2)) return;
+    const int l = idx % nl, i = idx / nl;
+    const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
+    if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) return;
+    fh_in[g.cell(i, j, k) * nl + l] += fh_out[g.cell(ti, tj, tk) * nl + l];
+}
+
+// drift adjoint preceded by the adjoint of the macrovars call that followed the
+// drift: fh_in(l, y) += fh_out(l, x) + d(rho, u)(x)/df_l^T (rhoh, uh, vh, wh)(x)
+// for x = y + c_l interior, where rho(x), u(x) are the macrovars outputs.  The
+// macrovars adjoints are taken at interior cells only.
+__global__ void k_ref_macro_drift_adj(float* fh_in, const float* fh_out, const float* rhoh, const float* uh,
+                                      const float* vh, const float* wh, const float* rho, const float* u,
+                                      const float* v, const float* w, RefGrid g) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    const int nl = g.nl;
+    if (idx >= nl * (g.nx + 2)) return;
+    const int l = idx % nl, i = idx / nl;
+    const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
+    if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) return;
+    const long long x = g.cell(ti, tj, tk);
+    const float inv = 1.0f / __ldg(rho + x);
+    const float ux = __ldg(u + x), uy = __ldg(v + x), uz = __ldg(w + x);
+    const float ax = __ldg(uh + x) * inv, ay = __ldg(vh + x) * inv, az = __ldg(wh + x) * inv;
+    const float m = __ldg(rhoh + x) + ax * ((float)c_cx[l] - ux) + ay * ((float)c_cy[l] - uy) + az * ((float)c_cz[l] - uz);
+    fh_in[g.cell(i, j, k) * nl + l] += fh_out[x * nl + l] + m;
+}
+
+// the interior of an adjoint array is consumed (drift overwrote it in the forward)
+__global__ void k_ref_zero_interior(float* fh, RefGrid g) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (idx >= g.nl * g.nx) return;
+    fh[g.cell(1, j, k) * g.nl + idx] = 0.0f;
+}
+
+// Accessor of the boundary adjoint: the forward copy this(ld,i,j,k) = s(ls,si,sj,sk)
+// becomes s^(ls,si,sj,sk) += this^(ld,i,j,k); this^(ld,i,j,k) = 0.  Within one
+// boundary kernel the copies have distinct sources, or share one only inside
+// the same thread (the inflow ghosts of a direction and its opposite), so the
+// accumulation needs no atomics; the kernels themselves run in reverse order.
+struct AdjAcc {
+    float* f;
+    RefGrid g;
+    __device__ __forceinline__ float* p(int l, int i, int j, int k) const { return f + g.cell(i, j, k) * g.nl + l; }
+    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const AdjAcc& s, int ls, int si, int sj,
+                                       int sk) const {
+        float* d = p(ld, i, j, k);
+        const float v = *d;
+        *d = 0.0f;
+        *s.p(ls, si, sj, sk) += v;
+    }
+};
+
+// reverse of k_inflow: outflow copies first (they ran last), then the inflow ghosts;
+// uvelh(k) receives d fghost / d uvel(k) times the ghosts' adjoints (a block is
+// one k: reduced over the block's threads, one atomic per warp).
+template <int Q>
+__global__ void __launch_bounds__(128) k_inflow_adj(AdjAcc f, float* uvelh, float rho0, float cosd, float sind) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int k = blockIdx.y + 1;
+    const int nx = f.g.nx;
+    float uh = 0.f;
+    if (j <= f.g.ny) {
+        float* out = f.p(0, nx + 1, j, k);
+        float* edge = f.p(0, nx, j, k);
+        float* gin = f.p(0, 0, j, k);
+        float* first = f.p(0, 1, j, k);
+        float vo[Q], vi[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            vo[l] = out[l];
+            vi[l] = gin[l];
+        }
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            out[l] = 0.0f;
+            gin[l] = 0.0f;
+            edge[l] += vo[l];
+        }
+        const float cs2 = 1.0f / 3.0f;
+        float acc[Q];
+#pragma unroll
+        for (int l = 0; l < Q; ++l) acc[l] = 0.0f;
+#pragma unroll
+        for (int l = 0; l < Q; ++l) {
+            const int s = (lat_cx(l) <= 0) ? l : lat_opposite(l);   // fghost(s) was stored at ghost l
+            acc[s] += vi[l];
+            uh -= vi[l] * 2.0f * lat_w<Q>(s) * rho0 * ((float)lat_cx(s) * cosd + (float)lat_cy(s) * sind) / cs2;
+        }
+#pragma unroll
+        for (int l = 0; l < Q; ++l)
+            if (lat_cx(l) <= 0) first[l] += acc[l];   // only directions with cx <= 0 are sources
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) uh += __shfl_down_sync(0xffffffffu, uh, o);
+    if ((threadIdx.x & 31) == 0 && uh != 0.0f) atomicAdd(uvelh + (k - 1), uh);
+}
+
+}  // namespace lbm

@@ -1054,3 +1054,4 @@ int lbm_status(lbm_ctx* c, int32_t* flags) {
 }  // extern "C"
 
 #include "ensemble_host.cuh"
+#include "adjoint_host.cuh"

@@ -59,6 +59,34 @@ CHANNEL_Q19_SMALL = CHANNEL_Q27_SMALL.with_(name="turb_inflow_q19_256x128x128", 
 CITY_Q27 = CHANNEL_Q27.with_(name="city_q27_512x256x256", city=16)
 CITY_Q27_REDUCED = CITY_Q27.with_(name="city_q27_128x64x64", nx=128, ny=64, nz=64)
 
+# Adjoint workload: D3Q19 channel with a sphere of radius 16; the loss is the
+# misfit of u at 200 probes after 100 steps, checkpoints every 10 steps
+ADJOINT_Q19 = Workload("adjoint_q19_256x128x128", 256, 128, 128, 19, steps=100, sphere=(64, 64, 64, 16))
+
+
+def probe_cells(wl: "Workload", n: int, seed: int) -> np.ndarray:
+    """n seeded interior fluid cells (i, j, k), 1-based, distinct."""
+    rng = np.random.default_rng(seed + 4242)
+    blank = blanking(wl)
+    seen, out = set(), []
+    while len(out) < n:
+        c = (int(rng.integers(1, wl.nx + 1)), int(rng.integers(1, wl.ny + 1)), int(rng.integers(1, wl.nz + 1)))
+        if c in seen or (blank is not None and blank[c[2], c[1], c[0]] != 0):
+            continue
+        seen.add(c)
+        out.append(c)
+    return np.array(out, dtype=np.int64)
+
+
+def inflow_perturbation(nz: int, seed: int, amp: float, dtype=np.float32) -> np.ndarray:
+    """Smooth seeded noise over k = 1..nz with maximum |value| = amp: four sine
+    modes of decaying amplitude with seeded phases."""
+    rng = np.random.default_rng(seed + 777)
+    z = np.arange(nz) / max(nz - 1, 1)
+    s = sum(rng.standard_normal() * np.sin((q + 1) * np.pi * z + rng.uniform(0, 2 * np.pi)) / (q + 1) for q in range(4))
+    return (amp * s / np.abs(s).max()).astype(dtype)
+
+
 def ensemble_members(n: int = 64, seed: int = 0, nl: int = 19, storage_steps: int = 500) -> list:
     """Members of the batched-ensemble workload: sizes drawn from the seed with
     nx in [96, 192] and ny, nz in [48, 96], each a multiple of 8; each member has
@@ -77,7 +105,7 @@ def ensemble_members(n: int = 64, seed: int = 0, nl: int = 19, storage_steps: in
 
 
 WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL,
-                                 CITY_Q27, CITY_Q27_REDUCED)}
+                                 CITY_Q27, CITY_Q27_REDUCED, ADJOINT_Q19)}
 
 
 def initial_macro(wl: Workload, dtype=np.float32):

@@ -24,3 +24,15 @@ def test_city_mask_boxes_stand_on_the_floor():
     assert m[0].sum() == 0 and m[1].sum() > 0                # k ghost empty, boxes start at k = 1
     assert m[41:].sum() == 0                                 # heights at most 40 cells
     assert set(np.unique(m)) <= {0, 1}
+
+
+def test_probes_and_inflow_perturbation():
+    wl = W.ADJOINT_Q19
+    pr = W.probe_cells(wl, 200, 0)
+    assert pr.shape == (200, 3) and len({tuple(p) for p in pr}) == 200
+    m = W.blanking(wl)
+    assert all(m[k, j, i] == 0 for i, j, k in pr)
+    assert pr.min() >= 1 and (pr[:, 0] <= wl.nx).all() and (pr[:, 2] <= wl.nz).all()
+    d = W.inflow_perturbation(wl.nz, 1, 5e-3)
+    assert d.shape == (wl.nz,) and abs(np.abs(d).max() - 5e-3) < 1e-9
+    assert np.abs(np.diff(d)).max() < 5e-3 * 0.2          # smooth over k
