@@ -161,5 +161,65 @@ module lbm_b200_iface
          type(c_ptr), value :: ctx
          integer(c_int32_t) :: flags
       end function
+      integer(c_int) function lbm_set_kernel(ctx, which) bind(C, name="lbm_set_kernel")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx
+         integer(c_int32_t), value :: which
+      end function
+
+      ! ---- adjoints of the per-call entry points (no reference counterpart) -------------------
+      integer(c_int) function lbm_postcoll_adj(ctx, fhat, f, tau, rho, u, v, w, ablvisc, rhohat, uhat, vhat, what, &
+                                               blanking) bind(C, name="lbm_postcoll_adj")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, fhat, f, tau, rho, u, v, w, ablvisc, rhohat, uhat, vhat, what, blanking
+      end function
+      integer(c_int) function lbm_macrovars_adj(ctx, fhat, rhohat, uhat, vhat, what, f) bind(C, name="lbm_macrovars_adj")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, fhat, rhohat, uhat, vhat, what, f
+      end function
+      integer(c_int) function lbm_drift_adj(ctx, fhat_in, fhat_out) bind(C, name="lbm_drift_adj")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, fhat_in, fhat_out
+      end function
+      integer(c_int) function lbm_macrovars_drift_adj(ctx, fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w) &
+            bind(C, name="lbm_macrovars_drift_adj")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w
+      end function
+      integer(c_int) function lbm_boundarycond_adj(ctx, f1hat, f2hat, uvelhat) bind(C, name="lbm_boundarycond_adj")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f1hat, f2hat, uvelhat
+      end function
+
+      ! ---- batched ensemble (no reference counterpart) -------------------------------------
+      integer(c_int) function lbm_ensemble_create(ens, members, nmembers) bind(C, name="lbm_ensemble_create")
+         import :: c_ptr, c_int, c_int32_t, lbm_params
+         type(c_ptr), intent(out)        :: ens
+         type(lbm_params), intent(in)    :: members(*)
+         integer(c_int32_t), value       :: nmembers
+      end function
+      integer(c_int) function lbm_ensemble_destroy(ens) bind(C, name="lbm_ensemble_destroy")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ens
+      end function
+      integer(c_int) function lbm_ensemble_member(ens, m, ctx) bind(C, name="lbm_ensemble_member")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: m
+         type(c_ptr), intent(out)  :: ctx
+      end function
+      integer(c_int) function lbm_ensemble_step(ens, nsteps) bind(C, name="lbm_ensemble_step")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: nsteps
+      end function
+      integer(c_int) function lbm_ensemble_autotune(ens, trial_steps, variant, ms_per_step) &
+            bind(C, name="lbm_ensemble_autotune")
+         import :: c_ptr, c_int, c_int32_t, c_float
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: trial_steps
+         integer(c_int32_t)        :: variant
+         real(c_float)             :: ms_per_step(*)
+      end function
    end interface
 end module lbm_b200_iface
