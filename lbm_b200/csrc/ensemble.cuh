@@ -4,10 +4,10 @@
 // state (its own buffers, boundaries, inflow, turbulence fields and step
 // counter) in the folded configuration.  The step of every member runs in one
 // launch of k_ens_step and the boundaries of every member in one launch of
-// k_ens_bc.  The blocks of a launch are dealt out member by member: member m
-// owns blocks prefix[m] .. prefix[m+1]-1, so a block never straddles two
-// members.  A block finds its member by a binary search over the prefix table,
-// copies that member's StepArgs into shared memory and then runs the same
+// k_ens_bc.  The blocks of a launch are dealt out member by member, so a block
+// never straddles two members.  A block reads its (member, block within the
+// member) from a per-launch table (one load, no search), copies that member's
+// StepArgs into shared memory and then runs the same
 // per-pair (pair_cell) or per-block (bc_fold_block) code as the single-state
 // kernels, so a member of an ensemble computes exactly what it computes alone.
 //
@@ -28,20 +28,8 @@ struct EnsMember {
 
 struct EnsLayout {
     const EnsMember* mem;
-    const int* prefix;   // [nm + 1] first block of each member in this launch's grid
-    int nm;
+    const int2* blk;     // per block of this launch's grid: (member, block index within the member)
 };
-
-// member owning block b: the largest m with prefix[m] <= b
-__device__ __forceinline__ int ens_member_of(const int* prefix, int nm, int b) {
-    int lo = 0, hi = nm;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(prefix + mid) <= b) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
 
 // the member's arguments into shared memory (word copy; StepArgs is 8-byte aligned)
 __device__ __forceinline__ void ens_load_args(unsigned char* raw, const StepArgs* ga) {
@@ -54,13 +42,12 @@ __device__ __forceinline__ void ens_load_args(unsigned char* raw, const StepArgs
 template <int Q, typename S, int T, int MINB>
 __global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
     __shared__ __align__(16) unsigned char raw[sizeof(StepArgs)];
-    const int b = blockIdx.x;
-    const int m = ens_member_of(L.prefix, L.nm, b);
-    const EnsMember* em = L.mem + m;
+    const int2 mb = __ldg(L.blk + blockIdx.x);
+    const EnsMember* em = L.mem + mb.x;
     ens_load_args(raw, &em->a[parity]);
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
     const int hp = a.g.nx / 2;
-    const long long q = (long long)(b - __ldg(L.prefix + m)) * T + threadIdx.x;
+    const long long q = (long long)mb.y * T + threadIdx.x;
     if (q >= (long long)hp * a.g.ny * a.g.nz) return;
     const int row = (int)(q / hp);
     const int i = 2 * (int)(q - (long long)row * hp) + 1;
@@ -74,13 +61,12 @@ __global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_ens_bc(EnsLayout L, int parity) {
     __shared__ __align__(16) unsigned char raw[sizeof(StepArgs)];
-    const int b = blockIdx.x;
-    const int m = ens_member_of(L.prefix, L.nm, b);
-    const EnsMember* em = L.mem + m;
+    const int2 mb = __ldg(L.blk + blockIdx.x);
+    const EnsMember* em = L.mem + mb.x;
     ens_load_args(raw, &em->a[parity]);
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
     bc_fold_block<Q, S>(reinterpret_cast<S*>(em->buf[1 - parity]), reinterpret_cast<const S*>(em->buf[parity]), a,
-                        em->nface_blocks, b - __ldg(L.prefix + m));
+                        em->nface_blocks, mb.y);
 }
 
 }  // namespace lbm

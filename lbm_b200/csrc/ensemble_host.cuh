@@ -28,7 +28,8 @@ struct lbm_ensemble {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     EnsMember* d_mem = nullptr;
     std::vector<EnsMember> h_mem;
-    int* d_prefix = nullptr;         // [LBM_ENS_VARIANTS + 1][nm + 1]: step grids per variant, then the boundary grid
+    int2* d_blk = nullptr;           // per block (member, block within member): step grids per variant, then boundaries
+    size_t blk_off[LBM_ENS_VARIANTS + 1] = {0, 0, 0, 0};
     int nblk[LBM_ENS_VARIANTS + 1] = {0, 0, 0, 0};
     int variant = 1;
     int graph_steps = LBM_ENS_GRAPH_STEPS;
@@ -62,8 +63,7 @@ int emember(lbm_ensemble* e, int m, int rc) {
 EnsLayout ens_layout(const lbm_ensemble* e, int which) {
     EnsLayout L;
     L.mem = e->d_mem;
-    L.prefix = e->d_prefix + (size_t)which * (e->m.size() + 1);
-    L.nm = (int)e->m.size();
+    L.blk = e->d_blk + e->blk_off[which];
     return L;
 }
 
@@ -219,29 +219,29 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
         rc = echeck(e, cudaEventCreateWithFlags(&e->ev[q], cudaEventDisableTiming), "cudaEventCreate");
     if (rc == LBM_OK) {
         e->h_mem.resize(nm);
-        std::vector<int> pre((LBM_ENS_VARIANTS + 1) * (nm + 1), 0);
-        for (int v = 0; v <= LBM_ENS_VARIANTS; ++v) {
-            int* P = pre.data() + (size_t)v * (nm + 1);
-            long long tot = 0;
+        std::vector<int2> blk;
+        for (int v = 0; v <= LBM_ENS_VARIANTS && rc == LBM_OK; ++v) {
+            e->blk_off[v] = blk.size();
             for (size_t k = 0; k < nm; ++k) {
                 const SoaGrid& g = e->m[k]->sg;
-                P[k] = (int)tot;
+                long long nb;
                 if (v < LBM_ENS_VARIANTS) {
                     const long long pairs = (long long)(g.nx / 2) * g.ny * g.nz;
-                    tot += (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
+                    nb = (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
-                    tot += 2LL * g.ny * ((g.nx + 127) / 128) + ((long long)e->nl * g.ny * g.nz + 127) / 128;
+                    nb = 2LL * g.ny * ((g.nx + 127) / 128) + ((long long)e->nl * g.ny * g.nz + 127) / 128;
                 }
+                for (long long b = 0; b < nb; ++b) blk.push_back(make_int2((int)k, (int)b));
             }
+            const long long tot = (long long)(blk.size() - e->blk_off[v]);
             if (tot >= (1LL << 31)) rc = efail(e, LBM_ERR_UNSUPPORTED, "ensemble too large for one launch");
-            P[nm] = (int)tot;
             e->nblk[v] = (int)tot;
         }
         if (rc == LBM_OK) rc = echeck(e, cudaMalloc(&e->d_mem, nm * sizeof(EnsMember)), "cudaMalloc(ensemble)");
-        if (rc == LBM_OK) rc = echeck(e, cudaMalloc(&e->d_prefix, pre.size() * sizeof(int)), "cudaMalloc(ensemble)");
+        if (rc == LBM_OK) rc = echeck(e, cudaMalloc(&e->d_blk, blk.size() * sizeof(int2)), "cudaMalloc(ensemble)");
         if (rc == LBM_OK)
-            rc = echeck(e, cudaMemcpy(e->d_prefix, pre.data(), pre.size() * sizeof(int), cudaMemcpyHostToDevice),
+            rc = echeck(e, cudaMemcpy(e->d_blk, blk.data(), blk.size() * sizeof(int2), cudaMemcpyHostToDevice),
                         "ensemble layout");
     }
     if (rc != LBM_OK) {
@@ -262,7 +262,7 @@ int lbm_ensemble_destroy(lbm_ensemble* e) {
         if (v) cudaEventDestroy(v);
     if (e->stream) cudaStreamDestroy(e->stream);
     cudaFree(e->d_mem);
-    cudaFree(e->d_prefix);
+    cudaFree(e->d_blk);
     for (lbm_ctx* c : e->m) lbm_destroy(c);
     delete e;
     return LBM_OK;
