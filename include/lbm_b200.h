@@ -196,6 +196,16 @@ int lbm_conservation(lbm_ctx* ctx, double* out_host);
 int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
                               void* stream);
 
+/* inflow_turbulence_compute (m_inflow_turbulence_compute.F90:3-62 with the
+ * Gaussian-spectrum random fields of m_pseudo2D.F90:3-169): fills uu, vv, ww and,
+ * if not NULL, rr -- device arrays (ny, nz, 0:nrturb) -- with levels chained by
+ * AR(1) (correlation 0.98) and normalised to zero mean and unit standard deviation
+ * from level 1 on.  The random phases come from a counter-based hash of seed (the
+ * reference draws them from the compiler's random_number).  Synchronises the
+ * context's stream before it returns (it frees its temporaries). */
+int lbm_inflow_turbulence_compute(lbm_ctx* ctx, float* uu, float* vv, float* ww, float* rr, int32_t nrturb,
+                                  uint64_t seed);
+
 /* ---- adjoint (reverse-mode) kernels of the per-call path ----
  * No counterpart in the reference, which has no gradients.  Each entry point
  * takes the adjoint (gradient of a scalar loss) of a forward call's outputs and

@@ -85,6 +85,7 @@ SIGNATURES = {
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],
+    "lbm_inflow_turbulence_compute": [P, P, P, P, P, I, ctypes.c_uint64],
     "lbm_postcoll_adj": [P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "lbm_macrovars_adj": [P, P, P, P, P, P, P],
     "lbm_drift_adj": [P, P, P],

@@ -196,6 +196,13 @@ class Lbm:
         self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
         self._call("lbm_inflow_turbulence_apply", _ptr(f), _ptr(df))
 
+    def inflow_turbulence_compute(self, uu, vv, ww, nrturb, seed, rr=None):
+        """Fill uu, vv, ww (and rr) -- float32 (nrturb+1, nz, ny) -- with the inflow-turbulence levels."""
+        for t in (uu, vv, ww, rr):
+            self._chk(t, (nrturb + 1, self.p.nz, self.p.ny), name="turbulence field")
+        self._call("lbm_inflow_turbulence_compute", _ptr(uu), _ptr(vv), _ptr(ww), _ptr(rr), ctypes.c_int32(nrturb),
+                   ctypes.c_uint64(seed))
+
     # ---- adjoints of the per-call kernels (reverse mode) -------------------------------
     def postcoll_adj(self, fhat, f, rho, u, v, w, rhohat, uhat, vhat, what, tau=None, ablvisc=None, blanking=None):
         """fhat: adjoint of postcoll's output f in, of its input f out; rhohat..what incremented.

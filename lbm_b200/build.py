@@ -20,7 +20,7 @@ HEADER = os.path.join(ROOT, "include", "lbm_b200.h")
 NVCC_FLAGS = [
     "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
     "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
-    "-shared", "-cudart", "static",
+    "-shared", "-cudart", "static", "-lcufft",
 ]
 
 

@@ -1055,3 +1055,4 @@ int lbm_status(lbm_ctx* c, int32_t* flags) {
 
 #include "ensemble_host.cuh"
 #include "adjoint_host.cuh"
+#include "turbulence_host.cuh"
