@@ -128,6 +128,11 @@ int lbm_compute_f(lbm_ctx* ctx, float* f, const float* feq);
 int lbm_boundarycond(lbm_ctx* ctx, float* f1, float* f2, const float* uvel);
 
 /* solids(f,blanking)               m_solids.F90:3; blanking is logical(4) over the ghost-inclusive grid */
+/* call forcings_apply(f1,external_forcing,rho,u,v,w)    m_forcings_apply.F90:3-64
+ * external_forcing(3,0:nx+1,0:ny+1,0:nz+1): f += feq2(rho, u - F/rho) - feq2(rho, u) at
+ * interior cells with rho > 0 (main.F90:306, between postcoll and solids) */
+int lbm_forcings_apply(lbm_ctx* ctx, float* f, const float* external_forcing, const float* rho, const float* u,
+                       const float* v, const float* w);
 int lbm_solids(lbm_ctx* ctx, float* f, const int32_t* blanking);
 
 /* inflow_turbulence_forcing(rho,u,v,w,ampl,it,nrturb)  m_inflow_turbulence_forcing.F90:5.
@@ -159,6 +164,12 @@ int lbm_set_solids(lbm_ctx* ctx, const int32_t* blanking);
 int lbm_set_turbulence(lbm_ctx* ctx, const float* uu, const float* vv, const float* ww, int32_t nrturb, float ampl);
 /* inflow profile uvel(nz) (device pointer) used by boundarycond from the next step on */
 int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
+/* external_forcing(3,0:nx+1,0:ny+1,0:nz+1) of the fused step (main.F90:291-306), a device
+ * array the caller owns and updates between steps; it is read at every step, applied after
+ * the collision and before the solid swap.  NULL turns the forcing off.  It runs in the
+ * two-cells-per-thread kernel: lbm_step returns LBM_ERR_UNSUPPORTED where that kernel does not
+ * apply (ihrr = 0, odd nx, another lbm_set_kernel choice) and ensembles refuse forced members. */
+int lbm_set_forcing(lbm_ctx* ctx, const float* external_forcing);
 /* advance nsteps time steps */
 int lbm_step(lbm_ctx* ctx, int32_t nsteps);
 /* choose the steady step kernel (LBM_KERNEL_*); both give the same results to round-off */

@@ -161,6 +161,23 @@ module lbm_b200_iface
          type(c_ptr), value :: ctx
          integer(c_int32_t) :: flags
       end function
+      ! call forcings_apply(f1,external_forcing,rho,u,v,w)   m_forcings_apply.F90:3
+      integer(c_int) function lbm_forcings_apply(ctx, f, external_forcing, rho, u, v, w) &
+            bind(C, name="lbm_forcings_apply")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, external_forcing, rho, u, v, w
+      end function
+      integer(c_int) function lbm_set_forcing(ctx, external_forcing) bind(C, name="lbm_set_forcing")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, external_forcing
+      end function
+      integer(c_int) function lbm_inflow_turbulence_compute(ctx, uu, vv, ww, rr, nrturb, seed) &
+            bind(C, name="lbm_inflow_turbulence_compute")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t
+         type(c_ptr), value        :: ctx, uu, vv, ww, rr
+         integer(c_int32_t), value :: nrturb
+         integer(c_int64_t), value :: seed
+      end function
       integer(c_int) function lbm_set_kernel(ctx, which) bind(C, name="lbm_set_kernel")
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value        :: ctx

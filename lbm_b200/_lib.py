@@ -74,6 +74,8 @@ SIGNATURES = {
     "lbm_set_solids": [P, P],
     "lbm_set_turbulence": [P, P, P, P, I, F],
     "lbm_set_inflow": [P, P],
+    "lbm_set_forcing": [P, P],
+    "lbm_forcings_apply": [P, P, P, P, P, P, P],
     "lbm_step": [P, I],
     "lbm_set_kernel": [P, I],
     "lbm_step_host": [P, I, P, ctypes.POINTER(ctypes.c_int32)],

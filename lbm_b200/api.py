@@ -266,6 +266,19 @@ class Lbm:
         self._call("lbm_set_turbulence", _ptr(uu), _ptr(vv), _ptr(ww), ctypes.c_int32(nrturb),
                    ctypes.c_float(ampl))
 
+    def forcings_apply(self, f, external_forcing, rho, u, v, w):
+        """external_forcing: float32 (nz+2, ny+2, nx+2, 3), the reference's external_forcing(3,0:nx+1,...)."""
+        self._f(f)
+        self._chk(external_forcing, self.p.sshape + (3,), name="external_forcing")
+        self._s(rho, u, v, w)
+        self._call("lbm_forcings_apply", _ptr(f), _ptr(external_forcing), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+
+    def set_forcing(self, external_forcing):
+        """Fused-step forcing field (read at every step; keep the tensor alive), or None."""
+        self._chk(external_forcing, self.p.sshape + (3,), name="external_forcing")
+        self._force_ref = external_forcing
+        self._call("lbm_set_forcing", _ptr(external_forcing))
+
     def set_inflow(self, uvel):
         self._chk(uvel, (self.p.nz,), name="uvel")
         self._call("lbm_set_inflow", _ptr(uvel))

@@ -66,6 +66,7 @@ struct lbm_ctx {
     int nsm = 148;
     int kopt_lo = 0, kopt_hi = 0;
     float* d_uvel = nullptr;      // uvel(nz)
+    const float* force = nullptr; // caller's external_forcing(3,0:nx+1,0:ny+1,0:nz+1), read every step (lbm_set_forcing)
     float* d_abl = nullptr;       // ablvisc(nz), zero unless set
     int* d_it = nullptr;          // number of the step being computed
     int* d_status = nullptr;
@@ -371,6 +372,7 @@ StepArgs step_args(lbm_ctx* c) {
     a.edge = c->d_edge;
     a.full_sector = (c->p.nx % (32 / (int)c->elem)) == 0;
     a.xg_dst = c->d_xg[1 - c->cur];
+    a.force = c->force;
     {
         const SoaGrid& g = c->sg;
         const long long plane = (long long)g.pitch * (g.ny + 2);
@@ -418,6 +420,9 @@ dim3 pair_grid(const lbm_ctx* c) { return dim3((unsigned)((c->p.nx / 2 + 127) / 
 
 template <int Q, typename S>
 int step_one(lbm_ctx* c) {
+    if (c->force && !pair_ok(c))
+        return fail(c, LBM_ERR_UNSUPPORTED, "step: the fused external forcing runs in the two-cells-per-thread kernel "
+                                            "(LBM_KERNEL_PAIR, ihrr = 1, even nx >= 4); use lbm_forcings_apply per call");
     const SoaGrid& g = c->sg;
     dim3 grd((g.nx + 127) / 128, g.ny, g.nz);
     StepArgs a = step_args(c);
@@ -426,6 +431,11 @@ int step_one(lbm_ctx* c) {
         k_step<Q, S, false, false><<<grd, 128, 0, c->stream>>>(b, b, a);
         c->launches++;
         LBM_LAUNCHED(c, "collide");
+        if (c->force) {
+            k_force_state<Q, S><<<grd, 128, 0, c->stream>>>(b, a);
+            c->launches++;
+            LBM_LAUNCHED(c, "external forcing");
+        }
         c->state = ST_POST;
     } else if (c->fold) {
         const int nxt = 1 - c->cur;
@@ -433,7 +443,10 @@ int step_one(lbm_ctx* c) {
         if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
             LBM_TRY(tma_launch<Q, S, true>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
         } else if (pair_ok(c)) {
-            k_step_pair<Q, S, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            if (c->force)
+                k_step_pair<Q, S, true, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            else
+                k_step_pair<Q, S, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
             c->launches++;
             LBM_LAUNCHED(c, "fused step (pair)");
         } else {
@@ -460,7 +473,10 @@ int step_one(lbm_ctx* c) {
         if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
             LBM_TRY(tma_launch<Q, S, false>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
         } else if (pair_ok(c)) {
-            k_step_pair<Q, S, false><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            if (c->force)
+                k_step_pair<Q, S, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            else
+                k_step_pair<Q, S, false><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
             c->launches++;
             LBM_LAUNCHED(c, "fused step (pair)");
         } else {
@@ -741,6 +757,24 @@ int lbm_boundarycond(lbm_ctx* c, float* f1, float* f2, const float* uvel) {
     if (c->p.ibnd == 1) NEED(c, uvel);
     if (f1 == f2) return fail(c, LBM_ERR_ARG, "boundarycond: f1 and f2 must be distinct buffers");
     return c->p.nl == 27 ? bc_ref<27>(c, f1, f2, uvel) : bc_ref<19>(c, f1, f2, uvel);
+}
+
+int lbm_forcings_apply(lbm_ctx* c, float* f, const float* external_forcing, const float* rho, const float* u,
+                       const float* v, const float* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, external_forcing); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
+    if (c->p.nl == 27) k_ref_forcings_apply<27><<<grd, 128, 0, c->stream>>>(f, external_forcing, rho, u, v, w, c->rg);
+    else k_ref_forcings_apply<19><<<grd, 128, 0, c->stream>>>(f, external_forcing, rho, u, v, w, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "forcings_apply");
+    return LBM_OK;
+}
+
+int lbm_set_forcing(lbm_ctx* c, const float* external_forcing) {
+    if (!c) return LBM_ERR_ARG;
+    c->force = external_forcing;
+    return LBM_OK;
 }
 
 int lbm_solids(lbm_ctx* c, float* f, const int32_t* blanking) {

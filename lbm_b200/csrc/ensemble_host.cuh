@@ -138,6 +138,7 @@ int ens_align(lbm_ensemble* e, int* used) {
     for (size_t k = 0; k < e->m.size(); ++k) {
         lbm_ctx* c = e->m[k];
         if (c->state == ST_NONE) return efail(e, LBM_ERR_STATE, "member %d: no state imported", (int)k);
+        if (c->force) return efail(e, LBM_ERR_UNSUPPORTED, "member %d: the ensemble kernels take no external forcing", (int)k);
         if (c->state == ST_PRE) {
             LBM_TRY(emember(e, (int)k, step_dispatch(c)));
             pre = true;

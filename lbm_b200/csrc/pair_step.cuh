@@ -235,7 +235,7 @@ __device__ __forceinline__ float comp(f2 v, int c) { return c ? v.y : v.x; }
 // solid swap, stores and the edge copy of the folded boundaries.  (Variants that
 // moved the turbulence slice out of this kernel -- a one-cell post-pass, or a
 // captured FP32 copy finished by a second kernel -- measured slower on B200.)
-template <int Q, typename S, bool WRAP>
+template <int Q, typename S, bool WRAP, bool FORCE = false>
 __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, const StepArgs& a, long long o, int i,
                                             int j, int k) {
     Moments2 m = moments_rows2<Q>(fp);
@@ -274,6 +274,36 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
             else fp[l].x = t[l];
         }
     }
+    if constexpr (FORCE) {
+        // forcings_apply (m_forcings_apply_kernel.F90:47-213): f += feq2(rho, u - F/rho) - feq2(rho, u)
+        // with the pre-collision rho, u, applied before the solid swap (its odd part flips at solid cells)
+        const long long c0 = (long long)i + (long long)(a.g.nx + 2) * ((long long)j + (long long)(a.g.ny + 2) * k);
+        const float* F = a.force + 3 * c0;
+        const bool ok0 = rho.x > 0.0f, ok1 = rho.y > 0.0f;
+        const f2 dux = make_float2(ok0 ? -__ldg(F) / rho.x : 0.0f, ok1 ? -__ldg(F + 3) / rho.y : 0.0f);
+        const f2 duy = make_float2(ok0 ? -__ldg(F + 1) / rho.x : 0.0f, ok1 ? -__ldg(F + 4) / rho.y : 0.0f);
+        const f2 duz = make_float2(ok0 ? -__ldg(F + 2) / rho.x : 0.0f, ok1 ? -__ldg(F + 5) / rho.y : 0.0f);
+        const f2 two = bc2(2.0f);
+        const f2 dusq = fma2(dux, fma2(two, ux, dux), fma2(duy, fma2(two, uy, duy), mul2(duz, fma2(two, uz, duz))));
+        const float sc = store_scale<S>();
+        const f2 wr = mul2(bc2(sc), rho);
+        const f2 sg = make_float2(solid0 ? -1.0f : 1.0f, solid1 ? -1.0f : 1.0f);
+        const f2 m15 = mul2(bc2(-1.5f), dusq);
+        fp[0] = fma2(mul2(bc2(lat_w<Q>(0)), wr), m15, fp[0]);
+#pragma unroll
+        for (int l = 1; l < Q; l += 2) {
+            const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+            f2 cu = bc2(0.f), dcu = bc2(0.f);
+            if (cx) { cu = cx > 0 ? add2(cu, ux) : sub2(cu, ux); dcu = cx > 0 ? add2(dcu, dux) : sub2(dcu, dux); }
+            if (cy) { cu = cy > 0 ? add2(cu, uy) : sub2(cu, uy); dcu = cy > 0 ? add2(dcu, duy) : sub2(dcu, duy); }
+            if (cz) { cu = cz > 0 ? add2(cu, uz) : sub2(cu, uz); dcu = cz > 0 ? add2(dcu, duz) : sub2(dcu, duz); }
+            const f2 wl = mul2(bc2(lat_w<Q>(l)), wr);
+            const f2 dE = mul2(wl, fma2(mul2(bc2(4.5f), dcu), fma2(two, cu, dcu), m15));
+            const f2 dO = mul2(mul2(sg, wl), mul2(bc2(3.0f), dcu));
+            fp[l] = add2(fp[l], add2(dE, dO));
+            fp[l + 1] = add2(fp[l + 1], sub2(dE, dO));
+        }
+    }
     S* q = dst + o;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
@@ -294,7 +324,7 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
 }
 
 // One pair (i, i+1), i odd, of row (j, k): pull, collide, store.
-template <int Q, typename S, bool WRAP>
+template <int Q, typename S, bool WRAP, bool FORCE = false>
 __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restrict__ dst, const StepArgs& a, int i, int j,
                                           int k) {
     const long long o = a.g.off(i, j, k);
@@ -306,7 +336,7 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
         const S* pym = (WRAP && j == a.g.ny) ? p0 - wrapd : p0;
         PairLoad<Q, S, 0>::run(fp, p0, pyp, pym, a);
     }
-    pair_update<Q, S, WRAP>(fp, dst, a, o, i, j, k);
+    pair_update<Q, S, WRAP, FORCE>(fp, dst, a, o, i, j, k);
 }
 
 #ifndef LBM_PAIR_MIN_BLOCKS
@@ -314,12 +344,12 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 #endif
 // Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
 // ihrr = 1, nx even and Q * dstride < 2^31.
-template <int Q, typename S, bool WRAP>
+template <int Q, typename S, bool WRAP, bool FORCE = false>
 __global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
                                                                         StepArgs a) {
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     if (i > a.g.nx) return;
-    pair_cell<Q, S, WRAP>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);
+    pair_cell<Q, S, WRAP, FORCE>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);
 }
 
 }  // namespace lbm

@@ -253,6 +253,45 @@ __global__ void k_ref_solids(float* f, const int32_t* blank, RefGrid g) {
     }
 }
 
+// forcings_apply: f += feq2(rho, u - F/rho) - feq2(rho, u) at interior cells with
+// rho > 0 (m_forcings_apply_kernel.F90:47-213; second-order equilibria), in the
+// closed form w rho [3 dcu + 4.5 dcu (2 cu + dcu) - 1.5 (2 u.du + du.du)].
+template <int Q>
+__global__ void __launch_bounds__(128) k_ref_forcings_apply(float* f, const float* force, const float* rho,
+                                                            const float* u, const float* v, const float* w, RefGrid g) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
+    const int n = min(128, g.nx + 1 - i0);
+    const int t = threadIdx.x;
+    if (n <= 0) return;
+    tile_load<Q>(sm, f, g.cell(i0, j, k), n);
+    __syncthreads();
+    if (t < n) {
+        const long long c = g.cell(i0 + t, j, k);
+        const float rr = rho[c];
+        if (rr > 0.0f) {
+            const float ux = u[c], uy = v[c], uz = w[c];
+            const float dux = -force[3 * c] / rr, duy = -force[3 * c + 1] / rr, duz = -force[3 * c + 2] / rr;
+            const float dusq = dux * (2.0f * ux + dux) + duy * (2.0f * uy + duy) + duz * (2.0f * uz + duz);
+            float* p = sm + t * Q;
+            p[0] += lat_w<Q>(0) * rr * (-1.5f * dusq);
+#pragma unroll
+            for (int l = 1; l < Q; l += 2) {
+                const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+                const float cu = cdot(cx, cy, cz, ux, uy, uz);
+                const float dcu = cdot(cx, cy, cz, dux, duy, duz);
+                const float wr = lat_w<Q>(l) * rr;
+                const float dE = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
+                const float dO = wr * 3.0f * dcu;
+                p[l] += dE + dO;
+                p[l + 1] += dE - dO;
+            }
+        }
+    }
+    __syncthreads();
+    tile_store<Q>(sm, f, g.cell(i0, j, k), n);
+}
+
 // inflow_turbulence_forcing: df(l,j,k) = feq(rho,u+ampl*uu) - feq(rho,u) at i = iturb
 // (m_inflow_turbulence_forcing.F90:44-128), evaluated as a difference of offsets
 template <int Q>

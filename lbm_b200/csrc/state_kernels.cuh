@@ -55,6 +55,7 @@ struct StepArgs {
     void* edge;               // post-collision populations at i=1 and i=nx: [side][l][k-1][j-1]
     int full_sector;          // x-ghost sectors hold nothing but the ghost and padding
     void* xg_dst;             // x-ghost columns of the buffer the step writes: [side][l][k-1][j-1]
+    const float* force;       // external_forcing(3,0:nx+1,0:ny+1,0:nz+1) or null (pair kernel only)
     // 32-bit element offsets of k_step_fast, computed on the host:
     int poff[27];             // pull source of direction l relative to the cell: l*dstride - (cx + cy*pitch + cz*plane)
     int soff[27];             // l*dstride
@@ -390,6 +391,42 @@ __global__ void __launch_bounds__(128, 8) k_step_fast(const S* __restrict__ src,
         Load32<Q, S, 0>::run(fp, p0, pyp, pym, a);
     }
     cell_update<Q, S, WRAP>(fp, dst, a, i, j, k);
+}
+
+// External forcing of the first step after an import, which collides in place
+// with the imported moments (k_step<Q,S,false,...>): adds feq2(rho, u - F/rho) -
+// feq2(rho, u) (m_forcings_apply_kernel.F90:47-213) with those moments.  The
+// solid swap already ran, so at solid cells the increment's odd part flips.
+template <int Q, typename S>
+__global__ void __launch_bounds__(128) k_force_state(S* f, StepArgs a) {
+    const SoaGrid g = a.g;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1;
+    const int k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    const long long c = (long long)i + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k);
+    const float rr = a.rho_in[c];
+    if (!(rr > 0.0f)) return;
+    const float ux = a.u_in[c], uy = a.v_in[c], uz = a.w_in[c];
+    const float dux = -a.force[3 * c] / rr, duy = -a.force[3 * c + 1] / rr, duz = -a.force[3 * c + 2] / rr;
+    const float dusq = dux * (2.0f * ux + dux) + duy * (2.0f * uy + duy) + duz * (2.0f * uz + duz);
+    const bool solid = a.solid ? a.solid[((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)] != 0 : false;
+    const long long o = g.off(i, j, k);
+    S* p0 = f + o;
+    p0[0] = Store<S>::from_f(Store<S>::to_f(p0[0]) + lat_w<Q>(0) * rr * (-1.5f * dusq));
+#pragma unroll
+    for (int l = 1; l < Q; l += 2) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        const float cu = cdot(cx, cy, cz, ux, uy, uz);
+        const float dcu = cdot(cx, cy, cz, dux, duy, duz);
+        const float wr = lat_w<Q>(l) * rr;
+        const float dE = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
+        const float dO = (solid ? -1.0f : 1.0f) * wr * 3.0f * dcu;
+        S* pl = f + (long long)l * g.dstride + o;
+        S* pm = f + (long long)(l + 1) * g.dstride + o;
+        *pl = Store<S>::from_f(Store<S>::to_f(*pl) + dE + dO);
+        *pm = Store<S>::from_f(Store<S>::to_f(*pm) + dE - dO);
+    }
 }
 
 // Advance the device step counter after the boundary kernels of a step.

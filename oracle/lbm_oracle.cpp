@@ -727,6 +727,47 @@ void turbulence_apply(const orc_params* p, T* f, const T* df) {
                 f[d.f(l, ip, j, k)] = f[d.f(l, ip, j, k)] + df[l + (long)d.nl * ((j - 1) + (long)d.ny * (k - 1))];
 }
 
+// forcings_apply, m_forcings_apply_kernel.F90:47-213: at interior cells with
+// rho > 0, f += feq2(rho, u - F/rho) - feq2(rho, u), second-order equilibria
+// (the third-order terms are commented out in the reference).  F(3,0:nx+1,0:ny+1,0:nz+1).
+template <typename T>
+void forcings_apply(const orc_params* p, T* f, const T* F, const T* rho, const T* u, const T* v, const T* w) {
+    const Dims d(p);
+    const Lattice<T> L(d.nl);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= d.nz; ++k)
+        for (int j = 1; j <= d.ny; ++j)
+            for (int i = 1; i <= d.nx; ++i) {
+                const long c = d.s(i, j, k);
+                const T rr = rho[c];
+                if (rr <= T(0.0)) continue;
+                const T vel0[3] = {u[c], v[c], w[c]};
+                const T du = -F[3 * c] / rr, dv = -F[3 * c + 1] / rr, dw = -F[3 * c + 2] / rr;
+                const T vel1[3] = {vel0[0] + du, vel0[1] + dv, vel0[2] + dw};
+                T A0[3][3], A1[3][3];
+                for (int q = 0; q < 3; ++q)
+                    for (int pp = 0; pp < 3; ++pp) {
+                        A0[q][pp] = rr * vel0[pp] * vel0[q] * L.inv2cs4;
+                        A1[q][pp] = rr * vel1[pp] * vel1[q] * L.inv2cs4;
+                    }
+                for (int l = 0; l < d.nl; ++l) {
+                    T cu = T(L.cx[l]) * vel0[0] + T(L.cy[l]) * vel0[1] + T(L.cz[l]) * vel0[2];
+                    T tmp1 = rr * (T(1.0) + cu * L.inv1cs2);
+                    T tmp2 = T(0.0);
+                    for (int q = 0; q < 3; ++q)
+                        for (int pp = 0; pp < 3; ++pp) tmp2 = tmp2 + L.H2[l][q][pp] * A0[q][pp];
+                    const T feq0 = L.w[l] * (tmp1 + tmp2 + T(0.0));
+                    cu = T(L.cx[l]) * vel1[0] + T(L.cy[l]) * vel1[1] + T(L.cz[l]) * vel1[2];
+                    tmp1 = rr * (T(1.0) + cu * L.inv1cs2);
+                    tmp2 = T(0.0);
+                    for (int q = 0; q < 3; ++q)
+                        for (int pp = 0; pp < 3; ++pp) tmp2 = tmp2 + L.H2[l][q][pp] * A1[q][pp];
+                    const T feq1 = L.w[l] * (tmp1 + tmp2 + T(0.0));
+                    f[d.f(l, i, j, k)] = f[d.f(l, i, j, k)] + (feq1 - feq0);
+                }
+            }
+}
+
 // fillghosts, m_fillghosts.F90:18-29
 template <typename T>
 void fillghosts(const orc_params* p, T* f) {
@@ -760,7 +801,8 @@ void init(const orc_params* p, T* fA, T* fB, const T* rho, const T* u, const T* 
 // On return fA holds f1 and fB holds f2 of the reference after the last step.
 template <typename T>
 void run(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, const T* ablvisc,
-         const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0, int nsteps) {
+         const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0, int nsteps,
+         const T* force = nullptr) {
     const Dims d(p);
     T* f1 = fA;
     T* f2 = fB;
@@ -770,6 +812,7 @@ void run(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, co
         if (p->lturb) turbulence_forcing(p, df.data(), rho, u, v, w, uu, vv, ww, it);
         postcoll(p, f1, tau, rho, u, v, w, ablvisc);
         if (p->lturb) turbulence_apply(p, f1, df.data());
+        if (force) forcings_apply(p, f1, force, rho, u, v, w);   // main.F90:306
         if (p->lsolids) solids(p, f1, blanking);
         boundarycond(p, f1, f2, uvel);
         drift(p, f2, f1);
@@ -844,7 +887,13 @@ void orc_init_##S(const orc_params* p, T* fA, T* fB, const T* rho, const T* u, c
 void orc_run_##S(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, const T* ablvisc,       \
                  const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0,       \
                  int nsteps) {                                                                                  \
-    run<T>(p, fA, fB, rho, u, v, w, tau, ablvisc, blanking, uvel, uu, vv, ww, it0, nsteps); }
+    run<T>(p, fA, fB, rho, u, v, w, tau, ablvisc, blanking, uvel, uu, vv, ww, it0, nsteps); }                  \
+void orc_run_forced_##S(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, const T* ablvisc,\
+                        const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0,\
+                        int nsteps, const T* force) {                                                          \
+    run<T>(p, fA, fB, rho, u, v, w, tau, ablvisc, blanking, uvel, uu, vv, ww, it0, nsteps, force); }           \
+void orc_forcings_apply_##S(const orc_params* p, T* f, const T* force, const T* rho, const T* u, const T* v,   \
+                            const T* w) { forcings_apply<T>(p, f, force, rho, u, v, w); }
 
 ORC_DEF(float, f32)
 ORC_DEF(double, f64)

@@ -65,7 +65,12 @@ void orc_turbulence_apply_##S(const orc_params* p, T* f, const T* df); \
 void orc_fillghosts_##S(const orc_params* p, T* f); \
 void orc_init_##S(const orc_params* p, T* fA, T* fB, const T* rho, const T* u, const T* v, const T* w, const T* uvel); \
 void orc_run_##S(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, const T* ablvisc, \
-                 const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0, int nsteps);
+                 const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0, int nsteps); \
+void orc_run_forced_##S(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, const T* ablvisc, \
+                        const int32_t* blanking, const T* uvel, const T* uu, const T* vv, const T* ww, int it0, \
+                        int nsteps, const T* force); \
+void orc_forcings_apply_##S(const orc_params* p, T* f, const T* force, const T* rho, const T* u, const T* v, \
+                            const T* w);
 
 ORC_DECL(float, f32)
 ORC_DECL(double, f64)

@@ -186,19 +186,28 @@ class Oracle:
         self._chk(fA, fB, rho, u, v, w, uvel)
         self._fn("init")(self._pp, _ptr(fA), _ptr(fB), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(uvel))
 
+    def forcings_apply(self, f, force, rho, u, v, w):
+        """force: (nz+2, ny+2, nx+2, 3), the reference's external_forcing(3,0:nx+1,0:ny+1,0:nz+1)."""
+        self._chk(f, force, rho, u, v, w)
+        self._fn("forcings_apply")(self._pp, _ptr(f), _ptr(force), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+
     def run(self, fA, fB, rho, u, v, w, tau, uvel, nsteps, it0=0, blanking=None, uu=None, vv=None, ww=None,
-            ablvisc=None):
-        """Time loop of main.F90:283-329; on return fA is f1 and fB is f2."""
+            ablvisc=None, force=None):
+        """Time loop of main.F90:283-329; on return fA is f1 and fB is f2.  force: a fixed
+        external_forcing applied every step (main.F90:306), or None."""
         if ablvisc is None:
             ablvisc = np.zeros(self.cfg.nz, self.dtype)
         if self.cfg.lsolids and blanking is None:
             raise ValueError("lsolids needs a blanking mask")
         if self.cfg.lturb and uu is None:
             raise ValueError("lturb needs uu, vv, ww")
-        self._chk(fA, fB, rho, u, v, w, tau, uvel, ablvisc, uu, vv, ww)
-        self._fn("run")(self._pp, _ptr(fA), _ptr(fB), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(tau),
-                        _ptr(ablvisc), _ptr(blanking), _ptr(uvel), _ptr(uu), _ptr(vv), _ptr(ww),
-                        ctypes.c_int(it0), ctypes.c_int(nsteps))
+        self._chk(fA, fB, rho, u, v, w, tau, uvel, ablvisc, uu, vv, ww, force)
+        args = [self._pp, _ptr(fA), _ptr(fB), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(tau), _ptr(ablvisc),
+                _ptr(blanking), _ptr(uvel), _ptr(uu), _ptr(vv), _ptr(ww), ctypes.c_int(it0), ctypes.c_int(nsteps)]
+        if force is None:
+            self._fn("run")(*args)
+        else:
+            self._fn("run_forced")(*args, _ptr(force))
 
 
 def tables(nl: int, dtype=np.float32):

@@ -152,3 +152,28 @@ def test_vreman_zero_fneq_gives_molecular_tau():
     s = (slice(1, -1),) * 3
     # fneq is pure round-off here; nu_t must stay far below nu
     assert np.all(np.abs(tau[s] - np.float32(3 * 1e-4 + 0.5)) < 2e-4)
+
+
+@pytest.mark.parametrize("nl", [19, 27])
+def test_forcing_changes_momentum_by_minus_the_force(nl):
+    """forcings_apply (m_forcings_apply_kernel.F90): sum df = 0 and sum c df = rho du = -F
+    (second-order equilibria carry mass and momentum exactly); F = 0 changes nothing."""
+    cfg = O.Config(6, 5, 4, nl)
+    o = O.Oracle(cfg, np.float64)
+    rng = np.random.default_rng(2)
+    rho = 1.0 + 0.01 * rng.standard_normal(cfg.sshape)
+    u, v, w = (0.03 * rng.standard_normal(cfg.sshape) for _ in range(3))
+    f0 = rng.uniform(0.0, 0.1, cfg.fshape)
+    F = 1e-4 * rng.standard_normal(cfg.sshape + (3,))
+    f = f0.copy()
+    o.forcings_apply(f, F, rho, u, v, w)
+    t = O.tables(nl, np.float64)
+    c = np.stack([t["cx"], t["cy"], t["cz"]], 1).astype(np.float64)
+    inner = (slice(1, -1),) * 3
+    df = (f - f0)[inner]
+    np.testing.assert_allclose(df.sum(-1), 0.0, atol=1e-15)
+    np.testing.assert_allclose(df @ c, -F[inner], rtol=1e-9, atol=1e-16)
+    assert np.array_equal(f[0], f0[0])                     # ghost cells untouched
+    g = f0.copy()
+    o.forcings_apply(g, np.zeros_like(F), rho, u, v, w)
+    assert np.array_equal(g, f0)
