@@ -307,12 +307,12 @@ __global__ void k_ref_macro_drift_adj(float* fh_in, const float* fh_out, const f
     fh_in[g.cell(i, j, k) * nl + l] += fh_out[x * nl + l] + m;
 }
 
-// the interior of an adjoint array is consumed (drift overwrote it in the forward)
-__global__ void k_ref_zero_interior(float* fh, RefGrid g) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-    if (idx >= g.nl * g.nx) return;
-    fh[g.cell(1, j, k) * g.nl + idx] = 0.0f;
+// the interior of an adjoint array is consumed (drift overwrote it in the forward);
+// one block per row (j,k) of the interior, looping over its nx*nl floats
+__global__ void __launch_bounds__(256) k_ref_zero_interior(float* fh, RefGrid g) {
+    float* row = fh + g.cell(1, blockIdx.x + 1, blockIdx.y + 1) * g.nl;
+    const int n = g.nl * g.nx;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) row[e] = 0.0f;
 }
 
 // Accessor of the boundary adjoint: the forward copy this(ld,i,j,k) = s(ls,si,sj,sk)

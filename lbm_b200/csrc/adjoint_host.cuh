@@ -97,7 +97,7 @@ int lbm_drift_adj(lbm_ctx* c, float* fhat_in, float* fhat_out) {
     const int nl = c->p.nl;
     k_ref_drift_adj<<<dim3((nl * (c->p.nx + 2) + 127) / 128, c->p.ny + 2, c->p.nz + 2), 128, 0, c->stream>>>(
         fhat_in, fhat_out, c->rg);
-    k_ref_zero_interior<<<dim3((nl * c->p.nx + 127) / 128, c->p.ny, c->p.nz), 128, 0, c->stream>>>(fhat_out, c->rg);
+    k_ref_zero_interior<<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(fhat_out, c->rg);
     c->launches += 2;
     LBM_LAUNCHED(c, "drift adjoint");
     return LBM_OK;
@@ -113,7 +113,7 @@ int lbm_macrovars_drift_adj(lbm_ctx* c, float* fhat_in, float* fhat_out, const f
     const int nl = c->p.nl;
     k_ref_macro_drift_adj<<<dim3((nl * (c->p.nx + 2) + 127) / 128, c->p.ny + 2, c->p.nz + 2), 128, 0, c->stream>>>(
         fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w, c->rg);
-    k_ref_zero_interior<<<dim3((nl * c->p.nx + 127) / 128, c->p.ny, c->p.nz), 128, 0, c->stream>>>(fhat_out, c->rg);
+    k_ref_zero_interior<<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(fhat_out, c->rg);
     c->launches += 2;
     LBM_LAUNCHED(c, "macrovars + drift adjoint");
     return LBM_OK;
