@@ -289,22 +289,27 @@ __global__ void k_ref_drift_adj(float* fh_in, const float* fh_out, RefGrid g) {
 // drift: fh_in(l, y) += fh_out(l, x) + d(rho, u)(x)/df_l^T (rhoh, uh, vh, wh)(x)
 // for x = y + c_l interior, where rho(x), u(x) are the macrovars outputs.  The
 // macrovars adjoints are taken at interior cells only.
-__global__ void k_ref_macro_drift_adj(float* fh_in, const float* fh_out, const float* rhoh, const float* uh,
-                                      const float* vh, const float* wh, const float* rho, const float* u,
-                                      const float* v, const float* w, RefGrid g) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    const int nl = g.nl;
-    if (idx >= nl * (g.nx + 2)) return;
-    const int l = idx % nl, i = idx / nl;
-    const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
-    if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) return;
-    const long long x = g.cell(ti, tj, tk);
-    const float inv = 1.0f / __ldg(rho + x);
-    const float ux = __ldg(u + x), uy = __ldg(v + x), uz = __ldg(w + x);
-    const float ax = __ldg(uh + x) * inv, ay = __ldg(vh + x) * inv, az = __ldg(wh + x) * inv;
-    const float m = __ldg(rhoh + x) + ax * ((float)c_cx[l] - ux) + ay * ((float)c_cy[l] - uy) + az * ((float)c_cz[l] - uz);
-    fh_in[g.cell(i, j, k) * nl + l] += fh_out[x * nl + l] + m;
+template <int Q>
+__global__ void __launch_bounds__(256) k_ref_macro_drift_adj(float* fh_in, const float* fh_out, const float* rhoh,
+                                                             const float* uh, const float* vh, const float* wh,
+                                                             const float* rho, const float* u, const float* v,
+                                                             const float* w, RefGrid g) {
+    // one block per row (j,k) of the ghost-inclusive grid, looping over its (nx+2)*Q entries
+    const int j = blockIdx.x, k = blockIdx.y;
+    float* row = fh_in + g.cell(0, j, k) * Q;
+    const int n = Q * (g.nx + 2);
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        const int l = idx % Q, i = idx / Q;
+        const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
+        if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) continue;
+        const long long x = g.cell(ti, tj, tk);
+        const float inv = 1.0f / __ldg(rho + x);
+        const float ux = __ldg(u + x), uy = __ldg(v + x), uz = __ldg(w + x);
+        const float ax = __ldg(uh + x) * inv, ay = __ldg(vh + x) * inv, az = __ldg(wh + x) * inv;
+        const float m =
+            __ldg(rhoh + x) + ax * ((float)c_cx[l] - ux) + ay * ((float)c_cy[l] - uy) + az * ((float)c_cz[l] - uz);
+        row[idx] += fh_out[x * Q + l] + m;
+    }
 }
 
 // the interior of an adjoint array is consumed (drift overwrote it in the forward);

@@ -111,8 +111,13 @@ int lbm_macrovars_drift_adj(lbm_ctx* c, float* fhat_in, float* fhat_out, const f
     NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
     if (fhat_in == fhat_out) return fail(c, LBM_ERR_ARG, "macrovars_drift_adj: the two adjoint arrays must be distinct");
     const int nl = c->p.nl;
-    k_ref_macro_drift_adj<<<dim3((nl * (c->p.nx + 2) + 127) / 128, c->p.ny + 2, c->p.nz + 2), 128, 0, c->stream>>>(
-        fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w, c->rg);
+    const dim3 grd(c->p.ny + 2, c->p.nz + 2);
+    if (nl == 27)
+        k_ref_macro_drift_adj<27><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w,
+                                                             c->rg);
+    else
+        k_ref_macro_drift_adj<19><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w,
+                                                             c->rg);
     k_ref_zero_interior<<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(fhat_out, c->rg);
     c->launches += 2;
     LBM_LAUNCHED(c, "macrovars + drift adjoint");

@@ -693,8 +693,8 @@ int lbm_drift(lbm_ctx* c, float* f, const float* feq) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, feq);
     if (f == feq) return fail(c, LBM_ERR_ARG, "drift: f and feq must be distinct buffers");
-    dim3 grd((c->p.nl * c->p.nx + 255) / 256, c->p.ny, c->p.nz);
-    k_ref_drift<<<grd, 256, 0, c->stream>>>(f, feq, c->rg);
+    if (c->p.nl == 27) k_ref_drift<27><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
+    else k_ref_drift<19><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
     c->launches++;
     LBM_LAUNCHED(c, "drift");
     return LBM_OK;

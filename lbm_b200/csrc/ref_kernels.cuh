@@ -132,13 +132,16 @@ __global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, cons
 
 // drift: f(l,i,j,k) = feq(l,i-cx,j-cy,k-cz) over interior cells; a thread per
 // (l,i) of a row, as m_drift_kernel.F90:62-84 flattens it
-__global__ void k_ref_drift(float* f, const float* feq, RefGrid g) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-    const int nl = g.nl;
-    if (idx >= nl * g.nx) return;
-    const int l = idx % nl, i = idx / nl + 1;
-    f[g.cell(i, j, k) * nl + l] = feq[g.cell(i - c_cx[l], j - c_cy[l], k - c_cz[l]) * nl + l];
+template <int Q>
+__global__ void __launch_bounds__(256) k_ref_drift(float* f, const float* feq, RefGrid g) {
+    // one block per interior row (j,k), looping over its nx*Q outputs
+    const int j = blockIdx.x + 1, k = blockIdx.y + 1;
+    float* out = f + g.cell(1, j, k) * Q;
+    const int n = Q * g.nx;
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        const int l = idx % Q, i = idx / Q + 1;
+        out[idx] = feq[g.cell(i - c_cx[l], j - c_cy[l], k - c_cz[l]) * Q + l];
+    }
 }
 
 // macrovars over the ghost-inclusive grid, summation order of m_macrovars_kernel.F90:175-187
