@@ -380,6 +380,8 @@ StepArgs step_args(lbm_ctx* c) {
             const long long d = lat_cx(l) + (long long)lat_cy(l) * g.pitch + (long long)lat_cz(l) * plane;
             a.poff[l] = (int)((long long)l * g.dstride - d);
             a.soff[l] = (int)((long long)l * g.dstride);
+            a.poffb[l] = (long long)a.poff[l] * (long long)c->elem;
+            a.soffb[l] = (long long)a.soff[l] * (long long)c->elem;
         }
     }
     return a;

@@ -206,7 +206,7 @@ __device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2
 template <int Q, typename S, int L>
 struct PairLoad {
     static __device__ __forceinline__ void run(f2 (&fp)[Q], const S* p0, const S* pyp, const S* pym, const StepArgs& a) {
-        const S* b = (lat_cy(L) > 0 ? pyp : (lat_cy(L) < 0 ? pym : p0)) + a.poff[L];
+        const S* b = reinterpret_cast<const S*>(reinterpret_cast<const char*>(lat_cy(L) > 0 ? pyp : (lat_cy(L) < 0 ? pym : p0)) + a.poffb[L]);
         if constexpr (sizeof(S) == 4) {
             if constexpr (lat_cx(L) == 0) fp[L] = __ldg(reinterpret_cast<const float2*>(b));
             else fp[L] = make_float2(__ldg(reinterpret_cast<const float*>(b)), __ldg(reinterpret_cast<const float*>(b) + 1));
@@ -307,8 +307,9 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
     S* q = dst + o;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(q + a.soff[l]) = __floats2half2_rn(fp[l].x, fp[l].y);
-        else *reinterpret_cast<float2*>(q + a.soff[l]) = fp[l];
+        char* qb = reinterpret_cast<char*>(q) + a.soffb[l];
+        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
+        else *reinterpret_cast<float2*>(qb) = fp[l];
     }
     if (WRAP && (i == 1 || i + 1 == a.g.nx)) {
         // the boundary kernel builds the inflow/outflow ghosts from these, read coalesced

@@ -59,6 +59,8 @@ struct StepArgs {
     // 32-bit element offsets of k_step_fast, computed on the host:
     int poff[27];             // pull source of direction l relative to the cell: l*dstride - (cx + cy*pitch + cz*plane)
     int soff[27];             // l*dstride
+    long long poffb[27];      // poff and soff in bytes, for the pair kernel: a 64-bit constant operand
+    long long soffb[27];      // per address instead of a sign-extended, scaled 32-bit offset
 };
 
 __device__ __forceinline__ void flag_bad_density(int* status, float rho, float ux, float uy, float uz) {
