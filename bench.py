@@ -528,6 +528,24 @@ def adjoint_bench(a):
     gnorm_f, gnorm_u = float(gf.double().norm()), float(gu.double().norm())
     pb.close()
     torch.cuda.empty_cache()
+    # the same gradient with the fused forward and the state-layout reverse sweep
+    from lbm_b200.adjoint import FusedProbeProblem
+    fb = FusedProbeProblem(p, probes, wl.steps, blanking=blank, checkpoint=10)
+    fb.forward(f1, f2, uvel)
+    fb.backward(torch.zeros(len(probes), 3, device="cuda"))
+    torch.cuda.synchronize()
+    s0, s1, s2 = ev(), ev(), ev()
+    s0.record()
+    us = fb.forward(f1, f2, uvel)
+    s1.record()
+    sf, su = fb.backward(2.0 * (us - truth))
+    s2.record()
+    torch.cuda.synchronize()
+    ts_fwd, ts_bwd = s0.elapsed_time(s1), s1.elapsed_time(s2)
+    agree = float((sf - gf).abs().max() / gf.abs().max())
+    fb.close()
+    del sf, su
+    torch.cuda.empty_cache()
     # the fused forward for the same steps, for scale
     s = Solver(p, rho, u, v, w, uvel, blanking=blank)
     s.step(3)
@@ -550,6 +568,13 @@ def adjoint_bench(a):
                        "target": "same run with uvel + 5e-3 smooth seeded noise"},
             "forward_ms": round(t_fwd, 2), "reverse_ms": round(t_bwd, 2),
             "fused_forward_ms": round(t_fused, 2), "reverse_over_fused_forward": round(t_bwd / t_fused, 3),
+            "state_layout_sweep": {"forward_ms": round(ts_fwd, 2), "reverse_ms": round(ts_bwd, 2),
+                                   "reverse_over_forward": round(ts_bwd / ts_fwd, 3),
+                                   "reverse_over_fused_forward": round(ts_bwd / t_fused, 3),
+                                   "gradient_vs_per_call_sweep": agree,
+                                   "how": "forward by the fused step with checkpoints (reference-layout export); "
+                                          "reverse replays each segment with the fused step and runs "
+                                          "lbm_state_adjoint_step"},
             "forward_mlups": round(cells * wl.steps / (t_fwd * 1e-3) / 1e6, 1),
             "loss": loss, "grad_norm": {"f1": gnorm_f, "uvel": gnorm_u},
             "gradient_check": "tests/test_gpu_adjoint.py: central FP64 differences, 8 seeded directions, rel <= 1e-4",

@@ -252,6 +252,29 @@ int lbm_macrovars_drift_adj(lbm_ctx* ctx, float* fhat_in, float* fhat_out, const
  * (incremented; needed when ibnd = 1), then zeroed */
 int lbm_boundarycond_adj(lbm_ctx* ctx, float* f1hat, float* f2hat, float* uvelhat);
 
+/* The same reverse sweep for forward runs made with the fused step.  The adjoint
+ * arrays are FP32 arrays of lbm_state_bytes bytes in the state's own layout
+ * with an explicit ghost shell (zero them before use).  FP32 state storage,
+ * ihrr = 1, no turbulence slice and no external forcing. */
+/* bytes of one state buffer (also the size of a state-layout adjoint array) */
+int lbm_state_bytes(lbm_ctx* ctx, int64_t* bytes);
+/* copy the newest state buffer (after an import: the imported f1; after a step:
+ * that step's post-collision populations with their ghosts) to dst */
+int lbm_state_copy(lbm_ctx* ctx, void* dst);
+/* one time step in reverse.  On entry W is the adjoint of f2 and A that of f1
+ * after the step; on exit W is the adjoint of f1 and A that of f2 before it.
+ * P: lbm_state_copy of the buffer the step started from -- pull = 1 when that
+ * was a stepped state (the step pulled from it), 0 when it was an import.
+ * uvelhat (nz) is incremented with the inflow profile's adjoint. */
+int lbm_state_adjoint_step(lbm_ctx* ctx, float* W, float* A, const void* P, int32_t pull, float* uvelhat);
+/* A += d(u, v, w at the probes)/df1^T uhat, with f1 = the reference's f1 after the
+ * step that produced P (lbm_state_copy); probes: nprobes (i, j, k) 1-based, uhat:
+ * nprobes x 3 (device arrays) */
+int lbm_state_adjoint_seed(lbm_ctx* ctx, float* A, const void* P, const int32_t* probes, const float* uhat,
+                           int32_t nprobes);
+/* a state-layout adjoint array to the reference layout f(nl,0:nx+1,0:ny+1,0:nz+1) */
+int lbm_state_adjoint_export(lbm_ctx* ctx, float* fhat, const float* A);
+
 /* ---- batched ensemble ----
  * No counterpart in the reference, which runs one domain per process (main.F90).
  * An ensemble holds many independent members of different sizes, each an

@@ -93,6 +93,11 @@ SIGNATURES = {
     "lbm_drift_adj": [P, P, P],
     "lbm_macrovars_drift_adj": [P, P, P, P, P, P, P, P, P, P, P],
     "lbm_boundarycond_adj": [P, P, P, P],
+    "lbm_state_bytes": [P, ctypes.POINTER(ctypes.c_int64)],
+    "lbm_state_copy": [P, P],
+    "lbm_state_adjoint_step": [P, P, P, P, I, P],
+    "lbm_state_adjoint_seed": [P, P, P, P, P, I],
+    "lbm_state_adjoint_export": [P, P, P],
     "lbm_ensemble_create": [ctypes.POINTER(P), ctypes.POINTER(LbmParams), I],
     "lbm_ensemble_destroy": [P],
     "lbm_ensemble_size": [P, ctypes.POINTER(ctypes.c_int32)],

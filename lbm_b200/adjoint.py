@@ -130,3 +130,80 @@ def initial_state(lbm: Lbm, rho, u, v, w, uvel):
     lbm.boundarycond(fB, fA, uvel)
     lbm.boundarycond(fA, fB, uvel)
     return fA, fB
+
+
+class FusedProbeProblem:
+    """The probe-misfit problem of :class:`ProbeProblem` with the forward run made
+    by the fused step (the library's default kernels) and the reverse sweep in
+    the state layout (``lbm_state_adjoint_*``).  Checkpoints are the
+    reference-layout (f1, f2) every ``checkpoint`` steps; each segment is
+    replayed from its checkpoint by importing it again (rho, u from macrovars),
+    keeping a copy of every step's state buffer."""
+
+    def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
+        if params.storage != "f32":
+            raise ValueError("the state-layout reverse sweep needs FP32 state storage")
+        self.p = params
+        self.lbm = Lbm(params)
+        self.nsteps = int(nsteps)
+        self.K = max(1, int(checkpoint))
+        self.blanking = blanking
+        self.probes = np.asarray(probes, dtype=np.int64)
+        self.probes_dev = torch.from_numpy(self.probes.astype(np.int32)).cuda()
+        self.pidx = torch.from_numpy((self.probes[:, 2] * (params.ny + 2) + self.probes[:, 1]) * (params.nx + 2)
+                                     + self.probes[:, 0]).cuda()
+        if blanking is not None:
+            self.lbm.set_solids(blanking)
+        self.ckpt = {}
+
+    def _import(self, f1, f2):
+        L = self.lbm
+        R = [L.empty_s() for _ in range(4)]
+        L.macrovars(*R, f1)
+        L.state_import(f1, f2, *R)
+        L.set_inflow(self.uvel)
+
+    def forward(self, f1, f2, uvel, keep: bool = True):
+        L = self.lbm
+        self.uvel = uvel.contiguous()
+        self.ckpt = {}
+        self._import(f1, f2)
+        for n in range(self.nsteps):
+            if keep and n % self.K == 0:
+                a, b = (f1.clone(), f2.clone()) if n == 0 else (L.empty_f(), L.empty_f())
+                if n > 0:
+                    L.state_export(a, b)
+                self.ckpt[n] = (a, b)
+            L.step(1)
+        R = [L.empty_s() for _ in range(4)]
+        L.get_macro(*R)
+        return torch.stack([R[q].reshape(-1)[self.pidx] for q in (1, 2, 3)], dim=1)
+
+    def backward(self, uhat_probes):
+        L = self.lbm
+        W, A = L.empty_state(), L.empty_state()
+        uvel_h = torch.zeros(self.p.nz, dtype=torch.float32, device="cuda")
+        for s in sorted(self.ckpt, reverse=True):
+            e = min(s + self.K, self.nsteps)
+            self._import(*self.ckpt[s])
+            D = L.state_scratch()
+            L.state_copy(D)                   # the imported f1: input of step s
+            P = []
+            for _ in range(s, e):
+                L.step(1)
+                P.append(L.state_scratch())
+                L.state_copy(P[-1])
+            if e == self.nsteps:
+                L.state_adjoint_seed(A, P[-1], self.probes_dev, uhat_probes.float())
+            for n in range(e - 1, s - 1, -1):
+                src = P[n - s - 1] if n > s else D
+                L.state_adjoint_step(W, A, src, n > s, uvel_h)
+                W, A = A, W                   # A: adjoint of f1 before step n, W: of f2
+            del P, D
+        g = L.empty_f()
+        L.state_adjoint_export(g, A)
+        return g, uvel_h
+
+    def close(self):
+        self.ckpt = {}
+        self.lbm.close()

@@ -234,6 +234,35 @@ class Lbm:
         self._chk(uvelhat, (self.p.nz,), name="uvelhat")
         self._call("lbm_boundarycond_adj", _ptr(f1hat), _ptr(f2hat), _ptr(uvelhat))
 
+    # ---- reverse sweep in the state layout ------------------------------------------------
+    def state_bytes(self) -> int:
+        n = ctypes.c_int64()
+        self._call("lbm_state_bytes", ctypes.byref(n))
+        return n.value
+
+    def empty_state(self):
+        """A zeroed FP32 array of one state buffer's size (a state copy or a state-layout adjoint)."""
+        return torch.zeros((self.state_bytes() + 3) // 4, dtype=torch.float32, device="cuda")
+
+    def state_scratch(self):
+        """An uninitialised FP32 array of one state buffer's size (for lbm_state_copy)."""
+        return torch.empty((self.state_bytes() + 3) // 4, dtype=torch.float32, device="cuda")
+
+    def state_copy(self, dst):
+        self._call("lbm_state_copy", _ptr(dst))
+
+    def state_adjoint_step(self, W, A, P, pull: bool, uvelhat):
+        self._call("lbm_state_adjoint_step", _ptr(W), _ptr(A), _ptr(P), ctypes.c_int32(1 if pull else 0), _ptr(uvelhat))
+
+    def state_adjoint_seed(self, A, P, probes, uhat):
+        """probes: int32 CUDA (n, 3) 1-based (i, j, k); uhat: float32 CUDA (n, 3)."""
+        self._call("lbm_state_adjoint_seed", _ptr(A), _ptr(P), _ptr(probes.contiguous()), _ptr(uhat.contiguous()),
+                   ctypes.c_int32(probes.shape[0]))
+
+    def state_adjoint_export(self, fhat, A):
+        self._f(fhat)
+        self._call("lbm_state_adjoint_export", _ptr(fhat), _ptr(A))
+
     def fillghosts(self, f):
         self._f(f)
         self._call("lbm_fillghosts", _ptr(f))

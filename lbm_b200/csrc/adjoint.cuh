@@ -341,28 +341,24 @@ struct AdjAcc {
 // reverse of k_inflow: outflow copies first (they ran last), then the inflow ghosts;
 // uvelh(k) receives d fghost / d uvel(k) times the ghosts' adjoints (a block is
 // one k: reduced over the block's threads, one atomic per warp).
-template <int Q>
-__global__ void __launch_bounds__(128) k_inflow_adj(AdjAcc f, float* uvelh, float rho0, float cosd, float sind) {
+template <int Q, typename Acc>
+__global__ void __launch_bounds__(128) k_inflow_adj(Acc f, float* uvelh, float rho0, float cosd, float sind) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y + 1;
     const int nx = f.g.nx;
     float uh = 0.f;
     if (j <= f.g.ny) {
-        float* out = f.p(0, nx + 1, j, k);
-        float* edge = f.p(0, nx, j, k);
-        float* gin = f.p(0, 0, j, k);
-        float* first = f.p(0, 1, j, k);
         float vo[Q], vi[Q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
-            vo[l] = out[l];
-            vi[l] = gin[l];
+            vo[l] = *f.p(l, nx + 1, j, k);
+            vi[l] = *f.p(l, 0, j, k);
         }
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
-            out[l] = 0.0f;
-            gin[l] = 0.0f;
-            edge[l] += vo[l];
+            *f.p(l, nx + 1, j, k) = 0.0f;
+            *f.p(l, 0, j, k) = 0.0f;
+            *f.p(l, nx, j, k) += vo[l];
         }
         const float cs2 = 1.0f / 3.0f;
         float acc[Q];
@@ -376,7 +372,7 @@ __global__ void __launch_bounds__(128) k_inflow_adj(AdjAcc f, float* uvelh, floa
         }
 #pragma unroll
         for (int l = 0; l < Q; ++l)
-            if (lat_cx(l) <= 0) first[l] += acc[l];   // only directions with cx <= 0 are sources
+            if (lat_cx(l) <= 0) *f.p(l, 1, j, k) += acc[l];   // only directions with cx <= 0 are sources
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) uh += __shfl_down_sync(0xffffffffu, uh, o);

@@ -3,46 +3,46 @@
 // boundary tables it uses.
 
 #include "adjoint.cuh"
+#include "adjoint_state.cuh"
 
 namespace {
 
 // boundarycond in reverse: the launches of run_bc in the opposite order, each
 // with the adjoint accessor (a copy becomes an accumulation into its source)
-template <int Q>
-int run_bc_adj(lbm_ctx* c, float* f1h, float* f2h, float* uvelh) {
+template <int Q, typename AdjA>
+int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
     const int nx = c->p.nx, ny = c->p.ny, nz = c->p.nz, nl = c->p.nl;
     cudaStream_t s = c->stream;
-    AdjAcc a1{f1h, c->rg}, a2{f2h, c->rg};
     auto periodic = [&](int axis) {
         dim3 grd;
         if (axis == 0) grd = dim3((ny + 2 + 127) / 128, nz + 2, nl);
         else if (axis == 1) grd = dim3((nx + 2 + 127) / 128, nz + 2, nl);
         else grd = dim3((nx + 2 + 127) / 128, ny + 2, nl);
-        k_periodic<AdjAcc><<<grd, 128, 0, s>>>(a1, axis, nl);
+        k_periodic<AdjA><<<grd, 128, 0, s>>>(a1, axis, nl);
         c->launches++;
     };
     const int codes[3] = {c->p.ibnd, c->p.jbnd, c->p.kbnd};
     for (int a = 2; a >= 0; --a)
         if (codes[a] == 0) periodic(a);
     if (c->p.ibnd == 1) {
-        k_inflow_adj<Q><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(a1, uvelh, c->p.rho0, c->cosd, c->sind);
+        k_inflow_adj<Q, AdjA><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(a1, uvelh, c->p.rho0, c->cosd, c->sind);
         c->launches++;
     }
     if (c->corners_on) {
-        k_corners<AdjAcc><<<1, 32, 0, s>>>(a1, a2, c->corners);
+        k_corners<AdjA><<<1, 32, 0, s>>>(a1, a2, c->corners);
         c->launches++;
     }
     for (int e = 2; e >= 0; --e) {
         if (!c->edges_on[e]) continue;
         const EdgeSet& es = c->edges[e];
-        k_edges<AdjAcc><<<dim3((es.nfree + 127) / 128, 4), 128, 0, s>>>(a1, a2, es);
+        k_edges<AdjA><<<dim3((es.nfree + 127) / 128, 4), 128, 0, s>>>(a1, a2, es);
         c->launches++;
     }
     for (int a = 2; a >= 0; --a) {
         if (!c->face_on[a]) continue;
         const int na = (a == 0) ? ny : nx;
         const int nb = (a == 2) ? ny : nz;
-        k_closed<AdjAcc><<<dim3((na + 127) / 128, nb, 2), 128, 0, s>>>(a1, a2, a, c->face[a][0], c->face[a][1], 1, 1);
+        k_closed<AdjA><<<dim3((na + 127) / 128, nb, 2), 128, 0, s>>>(a1, a2, a, c->face[a][0], c->face[a][1], 1, 1);
         c->launches++;
     }
     for (int a = 2; a >= 0; --a)
@@ -129,7 +129,88 @@ int lbm_boundarycond_adj(lbm_ctx* c, float* f1hat, float* f2hat, float* uvelhat)
     NEED(c, f1hat); NEED(c, f2hat);
     if (c->p.ibnd == 1) NEED(c, uvelhat);
     if (f1hat == f2hat) return fail(c, LBM_ERR_ARG, "boundarycond_adj: f1hat and f2hat must be distinct buffers");
-    return c->p.nl == 27 ? run_bc_adj<27>(c, f1hat, f2hat, uvelhat) : run_bc_adj<19>(c, f1hat, f2hat, uvelhat);
+    AdjAcc a1{f1hat, c->rg}, a2{f2hat, c->rg};
+    return c->p.nl == 27 ? run_bc_adj<27>(c, a1, a2, uvelhat) : run_bc_adj<19>(c, a1, a2, uvelhat);
+}
+
+// ---- the reverse sweep in the state layout --------------------------------------
+
+int lbm_state_bytes(lbm_ctx* c, int64_t* bytes) {
+    if (!c || !bytes) return LBM_ERR_ARG;
+    *bytes = (int64_t)((size_t)c->p.nl * c->sg.dstride * c->elem + 1024);
+    return LBM_OK;
+}
+
+int lbm_state_copy(lbm_ctx* c, void* dst) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, dst);
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "state_copy: no state imported");
+    const size_t n = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    return cuda_check(c, cudaMemcpyAsync(dst, c->buf[c->cur], n, cudaMemcpyDeviceToDevice, c->stream), "state_copy");
+}
+
+static int sadj_check(lbm_ctx* c, const char* what) {
+    if (c->p.storage != LBM_STORE_F32) return fail(c, LBM_ERR_UNSUPPORTED, "%s: FP32 state storage only", what);
+    if (c->p.ihrr != 1) return fail(c, LBM_ERR_UNSUPPORTED, "%s: the regularized collision (ihrr = 1) only", what);
+    if (c->nrturb > 0) return fail(c, LBM_ERR_UNSUPPORTED, "%s: no inflow-turbulence slice", what);
+    if (c->force) return fail(c, LBM_ERR_UNSUPPORTED, "%s: no external forcing", what);
+    return LBM_OK;
+}
+
+int lbm_state_adjoint_step(lbm_ctx* c, float* W, float* A, const void* P, int32_t pull, float* uvelhat) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, W); NEED(c, A); NEED(c, P);
+    if (c->p.ibnd == 1) NEED(c, uvelhat);
+    if (W == A) return fail(c, LBM_ERR_ARG, "state_adjoint_step: W and A must be distinct");
+    LBM_TRY(sadj_check(c, "state_adjoint_step"));
+    const SoaGrid& g = c->sg;
+    const int Q = c->p.nl;
+    const dim3 all((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), inner((g.nx + 127) / 128, g.ny, g.nz);
+    if (Q == 27) k_sadj_pull_t<27><<<all, 128, 0, c->stream>>>(W, A, g);
+    else k_sadj_pull_t<19><<<all, 128, 0, c->stream>>>(W, A, g);
+    c->launches++;
+    LBM_LAUNCHED(c, "state adjoint: drift");
+    SoaAdjAcc a1{W, g}, a2{A, g};
+    LBM_TRY(Q == 27 ? run_bc_adj<27>(c, a1, a2, uvelhat) : run_bc_adj<19>(c, a1, a2, uvelhat));
+    const int wrap = (c->p.jbnd == 0) ? 1 : 0;
+    const float* Pf = static_cast<const float*>(P);
+    if (Q == 27) {
+        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+    } else {
+        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+    }
+    c->launches++;
+    LBM_LAUNCHED(c, "state adjoint: collision");
+    return LBM_OK;
+}
+
+int lbm_state_adjoint_seed(lbm_ctx* c, float* A, const void* P, const int32_t* probes, const float* uhat,
+                           int32_t nprobes) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, A); NEED(c, P); NEED(c, probes); NEED(c, uhat);
+    if (nprobes < 1) return fail(c, LBM_ERR_ARG, "state_adjoint_seed: no probes");
+    LBM_TRY(sadj_check(c, "state_adjoint_seed"));
+    const int wrap = (c->p.jbnd == 0) ? 1 : 0;
+    const float* Pf = static_cast<const float*>(P);
+    if (c->p.nl == 27) k_sadj_seed<27><<<(nprobes + 127) / 128, 128, 0, c->stream>>>(A, Pf, c->sg, wrap, probes, uhat, nprobes);
+    else k_sadj_seed<19><<<(nprobes + 127) / 128, 128, 0, c->stream>>>(A, Pf, c->sg, wrap, probes, uhat, nprobes);
+    c->launches++;
+    LBM_LAUNCHED(c, "state adjoint: seed");
+    return LBM_OK;
+}
+
+int lbm_state_adjoint_export(lbm_ctx* c, float* fhat, const float* A) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, fhat); NEED(c, A);
+    const SoaGrid& g = c->sg;
+    const dim3 all((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2);
+    if (c->p.nl == 27) k_sadj_export<27><<<all, 128, 0, c->stream>>>(fhat, A, g);
+    else k_sadj_export<19><<<all, 128, 0, c->stream>>>(fhat, A, g);
+    c->launches++;
+    LBM_LAUNCHED(c, "state adjoint: export");
+    return LBM_OK;
 }
 
 }  // extern "C"

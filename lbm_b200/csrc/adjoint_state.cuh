@@ -1,0 +1,160 @@
+// adjoint_state.cuh -- the reverse sweep in the state (structure-of-arrays)
+// layout, for forward runs made with the fused step.
+//
+// The adjoints are FP32 arrays with the fused state's geometry (SoaGrid) and
+// an explicit ghost shell, i.e. the reference-layout arrays f1^, f2^ stored as
+// structure of arrays.  One reverse step is the per-call chain of adjoint.cuh
+// (drift, boundarycond, solids, postcoll, macrovars) with two differences: the
+// forward pre-collision populations are pulled from a copy of the fused state
+// buffer of the previous step, and the moments are those of the populations
+// themselves (the fused step takes rho, u from f), so the macrovars adjoint is
+// part of the cell kernel.  All accesses are coalesced: the transpose of the
+// pull is a shift by +c_l of each direction's block.
+#pragma once
+
+#include "adjoint.cuh"
+#include "state_kernels.cuh"
+
+namespace lbm {
+
+// boundary adjoint accessor on a state-layout FP32 array with explicit ghosts
+struct SoaAdjAcc {
+    float* f;
+    SoaGrid g;
+    __device__ __forceinline__ float* p(int l, int i, int j, int k) const {
+        return f + (long long)l * g.dstride + g.off(i, j, k);
+    }
+    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const SoaAdjAcc& s, int ls, int si, int sj,
+                                       int sk) const {
+        float* d = p(ld, i, j, k);
+        const float v = *d;
+        *d = 0.0f;
+        *s.p(ls, si, sj, sk) += v;
+    }
+};
+
+__device__ __forceinline__ bool interior(const SoaGrid& g, int i, int j, int k) {
+    return i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
+}
+
+// drift adjoint: W(l, y) += A(l, y + c_l) for every cell y whose target y + c_l is
+// interior, and A(l, y + c_l) = 0.  Each interior element of A is read by exactly
+// one thread, which also clears it.  Grid: x over i = 0..nx+1, y = j, z = k.
+template <int Q>
+__global__ void __launch_bounds__(128) k_sadj_pull_t(float* __restrict__ W, float* __restrict__ A, SoaGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i > g.nx + 1) return;
+    const long long o = g.off(i, j, k);
+    const long long plane = (long long)g.pitch * (g.ny + 2);
+    // all loads first, then the clears and accumulations: the compiler cannot tell
+    // that the directions' blocks do not overlap, so a per-direction
+    // load/clear/accumulate chain would run one memory round trip at a time
+    float v[Q];
+    bool in[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        in[l] = interior(g, i + lat_cx(l), j + lat_cy(l), k + lat_cz(l));
+        v[l] = in[l] ? A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane]
+                     : 0.0f;
+    }
+    float w[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) w[l] = W[(long long)l * g.dstride + o];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        if (!in[l]) continue;
+        A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane] = 0.0f;
+        W[(long long)l * g.dstride + o] = w[l] + v[l];
+    }
+}
+
+// postcoll (+solids, +the macrovars of its input) adjoint at interior cells: W
+// holds the adjoint of the post-collision populations and receives that of the
+// pre-collision ones.  PULL: the forward input is pull(P) (P a copy of the
+// previous step's fused state buffer, offsets f - w, FP32); otherwise it is P
+// itself (the state as imported).  wrap: periodic j without stored ghost rows.
+template <int Q, bool PULL>
+__global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const float* __restrict__ P, SoaGrid g,
+                                                   int wrap, const uint8_t* __restrict__ solid, CollideParams cp,
+                                                   const float* __restrict__ abl) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    const long long o = g.off(i, j, k);
+    float fp[Q], gh[Q], fh[Q];
+    if (PULL) {
+        PullMacro<Q, float, 0>::run(fp, P, g, o, j, wrap != 0);
+    } else {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) fp[l] = P[(long long)l * g.dstride + o];
+    }
+#pragma unroll
+    for (int l = 0; l < Q; ++l) gh[l] = W[(long long)l * g.dstride + o];
+    if (solid && solid[((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)]) {
+#pragma unroll
+        for (int l = 1; l + 1 < Q; l += 2) {
+            const float x = gh[l];
+            gh[l] = gh[l + 1];
+            gh[l + 1] = x;
+        }
+    }
+    const Moments m = moments<Q>(fp);
+    const float rho = 1.0f + m.s0;
+    const float ux = m.jx / rho, uy = m.jy / rho, uz = m.jz / rho;
+    float rh = 0.f, uxh = 0.f, uyh = 0.f, uzh = 0.f;
+    collide_adj<Q>(fp, gh, rho, ux, uy, uz, cp, abl ? abl[k - 1] : 0.0f, cp.tau0, fh, rh, uxh, uyh, uzh);
+    // rho = sum f, u = (sum c f) / rho
+    const float ax = uxh / rho, ay = uyh / rho, az = uzh / rho;
+    const float base = rh - (ax * ux + ay * uy + az * uz);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        float d = base;
+        macc(d, lat_cx(l), ax);
+        macc(d, lat_cy(l), ay);
+        macc(d, lat_cz(l), az);
+        W[(long long)l * g.dstride + o] = fh[l] + d;
+    }
+}
+
+// loss seed: A(l, x_p) += d(u, v, w)(x_p)/df_l^T uhat_p at the probe cells, where
+// f = pull(P) is the reference's f1 after the last step.  probes: (i, j, k)
+// triples, 1-based, distinct; uhat: (P, 3).
+template <int Q>
+__global__ void k_sadj_seed(float* A, const float* __restrict__ P, SoaGrid g, int wrap, const int* probes,
+                            const float* uhat, int np) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int i = probes[3 * p], j = probes[3 * p + 1], k = probes[3 * p + 2];
+    const long long o = g.off(i, j, k);
+    float fp[Q];
+    PullMacro<Q, float, 0>::run(fp, P, g, o, j, wrap != 0);
+    const Moments m = moments<Q>(fp);
+    const float rho = 1.0f + m.s0;
+    const float ux = m.jx / rho, uy = m.jy / rho, uz = m.jz / rho;
+    const float ax = uhat[3 * p] / rho, ay = uhat[3 * p + 1] / rho, az = uhat[3 * p + 2] / rho;
+    const float base = -(ax * ux + ay * uy + az * uz);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        float d = base;
+        macc(d, lat_cx(l), ax);
+        macc(d, lat_cy(l), ay);
+        macc(d, lat_cz(l), az);
+        A[(long long)l * g.dstride + o] += d;
+    }
+}
+
+// a state-layout adjoint to the reference layout (all cells, no weights: adjoints of
+// f and of f - w are the same)
+template <int Q>
+__global__ void k_sadj_export(float* __restrict__ ref, const float* __restrict__ A, SoaGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, k = blockIdx.z;
+    if (i > g.nx + 1) return;
+    const long long c = (long long)i + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k);
+    const long long o = g.off(i, j, k);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) ref[c * Q + l] = A[(long long)l * g.dstride + o];
+}
+
+}  // namespace lbm

@@ -240,7 +240,7 @@ def test_autograd_function_gives_the_sweep_gradient():
     u = pb.forward(f1, f2, uvel)
     r1, ru = pb.backward(2.0 * (u - target))
     assert torch.equal(g1, r1) and torch.equal(gu, ru)
-    assert float(loss) > 0 and float(gu.abs().sum()) > 0
+    assert float(loss.detach()) > 0 and float(gu.abs().sum()) > 0
     pb.close()
 
 
@@ -277,3 +277,55 @@ def test_fused_adjoints_equal_the_chained_ones():
     L.postcoll_adj(g1, F, *Rf, *h1)
     L.postcoll_adj(g2, F, *Rf, *h2, blanking=blank)
     assert torch.equal(g1, g2) and all(torch.equal(p, q) for p, q in zip(h1, h2))
+
+
+# ---- the reverse sweep in the state layout (forward by the fused step) -----------------
+def fused_problem(wl, checkpoint, spin_from):
+    from lbm_b200 import Params
+    from lbm_b200.adjoint import FusedProbeProblem
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=2,
+               kinevisc=wl.kinevisc)
+    blank = torch.from_numpy(W.blanking(wl)).cuda()
+    return FusedProbeProblem(p, W.probe_cells(wl, 24, 1), wl.steps, blanking=blank, checkpoint=checkpoint)
+
+
+@pytest.mark.parametrize("nl", [19, 27])
+def test_state_layout_sweep_matches_fp64_finite_differences(nl):
+    wl = CASE.with_(nl=nl)
+    pb, f1, f2, uvel = problem(wl, 5)           # spun-up initial state (per-call path)
+    fb = fused_problem(wl, 5, None)
+    truth = fb.forward(f1, f2, uvel + cuda(W.inflow_perturbation(wl.nz, 2, 5e-3)), keep=False)
+    fb.forward(f1, f2, uvel)
+    F1, F2, U, T = host(f1), host(f2), host(uvel), host(truth)
+    u64 = oracle_probe_u(wl, fb.probes, F1, F2, U)
+    gf, gu = fb.backward(cuda(2.0 * (u64 - T)))
+    gf, gu = host(gf), host(gu)
+    # the per-call sweep gives the same gradient
+    pb.forward(f1, f2, uvel)
+    rf, ru = (host(t) for t in pb.backward(cuda(2.0 * (u64 - T))))
+    assert np.abs(gf - rf).max() <= 1e-4 * np.abs(rf).max() and np.abs(gu - ru).max() <= 1e-4 * np.abs(ru).max()
+    rng = np.random.default_rng(43)
+    inner = (slice(1, -1),) * 3
+    for d in range(8):
+        df, du = np.zeros_like(F1), np.zeros_like(U)
+        if d < 4:
+            df[inner] = 1e-6 * rng.standard_normal(df[inner].shape)
+        else:
+            du = 1e-6 * rng.standard_normal(U.shape)
+        fd = (oracle_loss(wl, fb.probes, F1 + df, F2, U + du, T) - oracle_loss(wl, fb.probes, F1 - df, F2, U - du, T)) / 2
+        ad = float((gf * df).sum() + (gu * du).sum())
+        assert rel(fd, ad) < 1e-4, (d, fd, ad)
+    pb.close()
+    fb.close()
+
+
+def test_state_layout_sweep_refuses_unsupported_states():
+    from lbm_b200 import LbmError, Params
+    from lbm_b200.adjoint import FusedProbeProblem
+    with pytest.raises(ValueError):
+        FusedProbeProblem(Params(nx=8, ny=6, nz=6, nl=19, iturb_pos=2, storage="f16"), [(1, 1, 1)], 2)
+    from lbm_b200 import Lbm
+    L = Lbm(Params(nx=8, ny=6, nz=6, nl=19, iturb_pos=2, ihrr=0))
+    a, b = L.empty_state(), L.empty_state()
+    with pytest.raises(LbmError, match="ihrr"):
+        L.state_adjoint_step(a, b, a.clone(), True, torch.zeros(6, device="cuda"))
