@@ -208,6 +208,31 @@ module lbm_b200_iface
          type(c_ptr), value :: ctx, f1hat, f2hat, uvelhat
       end function
 
+      integer(c_int) function lbm_state_bytes(ctx, bytes) bind(C, name="lbm_state_bytes")
+         import :: c_ptr, c_int, c_int64_t
+         type(c_ptr), value   :: ctx
+         integer(c_int64_t)   :: bytes
+      end function
+      integer(c_int) function lbm_state_copy(ctx, dst) bind(C, name="lbm_state_copy")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, dst
+      end function
+      integer(c_int) function lbm_state_adjoint_step(ctx, w, a, p, pull, uvelhat) bind(C, name="lbm_state_adjoint_step")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx, w, a, p, uvelhat
+         integer(c_int32_t), value :: pull
+      end function
+      integer(c_int) function lbm_state_adjoint_seed(ctx, a, p, probes, uhat, nprobes) &
+            bind(C, name="lbm_state_adjoint_seed")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx, a, p, probes, uhat
+         integer(c_int32_t), value :: nprobes
+      end function
+      integer(c_int) function lbm_state_adjoint_export(ctx, fhat, a) bind(C, name="lbm_state_adjoint_export")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, fhat, a
+      end function
+
       ! ---- batched ensemble (no reference counterpart) -------------------------------------
       integer(c_int) function lbm_ensemble_create(ens, members, nmembers) bind(C, name="lbm_ensemble_create")
          import :: c_ptr, c_int, c_int32_t, lbm_params
