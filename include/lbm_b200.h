@@ -172,6 +172,17 @@ int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
 int lbm_set_forcing(lbm_ctx* ctx, const float* external_forcing);
 /* advance nsteps time steps */
 int lbm_step(lbm_ctx* ctx, int32_t nsteps);
+/* one time step whose result (the state buffer lbm_state_copy would give) is
+ * written to dst, device memory of lbm_state_bytes bytes, 256-byte aligned, that
+ * the caller owns, instead of to the context's other buffer.  The context reads
+ * the following step from dst, so dst must stay allocated until the context has
+ * stepped twice more or imported a state.  The first step after an import (a
+ * collision in place) is written to the context's buffer and copied to dst.
+ * Otherwise the ghost shell of the buffer the step would have overwritten is
+ * copied to dst first (the boundaries read ghost values of two steps before),
+ * so dst ends up holding what that buffer would.  Used to keep every state of
+ * a replayed segment without copying whole buffers. */
+int lbm_step_to(lbm_ctx* ctx, void* dst);
 /* choose the steady step kernel (LBM_KERNEL_*); both give the same results to round-off */
 int lbm_set_kernel(lbm_ctx* ctx, int32_t which);
 /* host-buffer step: copies uvel(nz) from host memory before each step (NULL keeps the
@@ -263,6 +274,9 @@ int lbm_state_bytes(lbm_ctx* ctx, int64_t* bytes);
 int lbm_state_copy(lbm_ctx* ctx, void* dst);
 /* one time step in reverse.  On entry W is the adjoint of f2 and A that of f1
  * after the step; on exit W is the adjoint of f1 and A that of f2 before it.
+ * The interior of W is not read on entry (the interior of f2 is overwritten by
+ * the next step's collision, so its adjoint is zero) and the interior of A is
+ * left as it was on exit (read as zero by the next call, which takes it as W).
  * P: lbm_state_copy of the buffer the step started from -- pull = 1 when that
  * was a stepped state (the step pulled from it), 0 when it was an import.
  * uvelhat (nz) is incremented with the inflow profile's adjoint. */

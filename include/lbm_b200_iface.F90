@@ -150,6 +150,10 @@ module lbm_b200_iface
          type(c_ptr), value        :: ctx
          integer(c_int32_t), value :: nsteps
       end function
+      integer(c_int) function lbm_step_to(ctx, dst) bind(C, name="lbm_step_to")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, dst
+      end function
       integer(c_int) function lbm_step_host(ctx, nsteps, uvel_host, status) bind(C, name="lbm_step_host")
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value        :: ctx, uvel_host

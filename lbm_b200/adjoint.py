@@ -138,7 +138,7 @@ class FusedProbeProblem:
     the state layout (``lbm_state_adjoint_*``).  Checkpoints are the
     reference-layout (f1, f2) every ``checkpoint`` steps; each segment is
     replayed from its checkpoint by importing it again (rho, u from macrovars),
-    keeping a copy of every step's state buffer."""
+    each step writing its state buffer into an array of its own (lbm_step_to)."""
 
     def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
         if params.storage != "f32":
@@ -190,9 +190,8 @@ class FusedProbeProblem:
             L.state_copy(D)                   # the imported f1: input of step s
             P = []
             for _ in range(s, e):
-                L.step(1)
                 P.append(L.state_scratch())
-                L.state_copy(P[-1])
+                L.step_to(P[-1])              # the step writes its state into P[-1]
             if e == self.nsteps:
                 L.state_adjoint_seed(A, P[-1], self.probes_dev, uhat_probes.float())
             for n in range(e - 1, s - 1, -1):

@@ -315,6 +315,11 @@ class Lbm:
     def step(self, nsteps=1):
         self._call("lbm_step", ctypes.c_int32(nsteps))
 
+    def step_to(self, dst):
+        """One step whose state buffer is written to ``dst`` (a :meth:`state_scratch`
+        tensor, kept alive by the caller until two more steps or an import)."""
+        self._call("lbm_step_to", _ptr(dst))
+
     def set_kernel(self, which: str):
         """Steady step kernel: "pair" (two cells per thread, default where it applies),
         "pull" (one cell per thread) or "tma" (shared-memory tiles)."""

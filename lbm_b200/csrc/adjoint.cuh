@@ -339,8 +339,10 @@ struct AdjAcc {
 };
 
 // reverse of k_inflow: outflow copies first (they ran last), then the inflow ghosts;
-// uvelh(k) receives d fghost / d uvel(k) times the ghosts' adjoints (a block is
-// one k: reduced over the block's threads, one atomic per warp).
+// uvelh(k) receives d fghost / d uvel(k) times the ghosts' adjoints (one atomic
+// per warp; launch with blocks of 32 threads over j, one k per block row).
+// Every value is loaded before the first store, so the accesses of a thread
+// overlap instead of running one read-modify-write at a time.
 template <int Q, typename Acc>
 __global__ void __launch_bounds__(128) k_inflow_adj(Acc f, float* uvelh, float rho0, float cosd, float sind) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -348,17 +350,13 @@ __global__ void __launch_bounds__(128) k_inflow_adj(Acc f, float* uvelh, float r
     const int nx = f.g.nx;
     float uh = 0.f;
     if (j <= f.g.ny) {
-        float vo[Q], vi[Q];
+        float vo[Q], vi[Q], on[Q], o1[Q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
             vo[l] = *f.p(l, nx + 1, j, k);
             vi[l] = *f.p(l, 0, j, k);
-        }
-#pragma unroll
-        for (int l = 0; l < Q; ++l) {
-            *f.p(l, nx + 1, j, k) = 0.0f;
-            *f.p(l, 0, j, k) = 0.0f;
-            *f.p(l, nx, j, k) += vo[l];
+            on[l] = *f.p(l, nx, j, k);
+            o1[l] = (lat_cx(l) <= 0 && nx > 1) ? *f.p(l, 1, j, k) : 0.0f;
         }
         const float cs2 = 1.0f / 3.0f;
         float acc[Q];
@@ -371,12 +369,99 @@ __global__ void __launch_bounds__(128) k_inflow_adj(Acc f, float* uvelh, float r
             uh -= vi[l] * 2.0f * lat_w<Q>(s) * rho0 * ((float)lat_cx(s) * cosd + (float)lat_cy(s) * sind) / cs2;
         }
 #pragma unroll
-        for (int l = 0; l < Q; ++l)
-            if (lat_cx(l) <= 0) *f.p(l, 1, j, k) += acc[l];   // only directions with cx <= 0 are sources
+        for (int l = 0; l < Q; ++l) {
+            *f.p(l, nx + 1, j, k) = 0.0f;
+            *f.p(l, 0, j, k) = 0.0f;
+            // the outflow copy's source (nx) first, then the inflow's (1); one cell when nx = 1
+            float a = on[l] + vo[l];
+            if (nx == 1 && lat_cx(l) <= 0) a += acc[l];
+            *f.p(l, nx, j, k) = a;
+            if (nx > 1 && lat_cx(l) <= 0) *f.p(l, 1, j, k) = o1[l] + acc[l];
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) uh += __shfl_down_sync(0xffffffffu, uh, o);
     if ((threadIdx.x & 31) == 0 && uh != 0.0f) atomicAdd(uvelh + (k - 1), uh);
+}
+
+// reverse of k_periodic (same grid): both ghost planes of the axis pass their
+// adjoints to the planes they were copied from; loads before stores.
+template <typename Acc>
+__global__ void k_periodic_adj(Acc a, int axis, int nl) {
+    const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
+    const int l = blockIdx.z;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (l >= nl) return;
+    int n;
+    float *g0, *g1, *sn, *s1;     // ghost 0, ghost n+1, their sources n and 1
+    if (axis == 0) {
+        if (t > ny + 1) return;
+        n = nx; g0 = a.p(l, 0, t, s); g1 = a.p(l, nx + 1, t, s); sn = a.p(l, nx, t, s); s1 = a.p(l, 1, t, s);
+    } else if (axis == 1) {
+        if (t > nx + 1) return;
+        n = ny; g0 = a.p(l, t, 0, s); g1 = a.p(l, t, ny + 1, s); sn = a.p(l, t, ny, s); s1 = a.p(l, t, 1, s);
+    } else {
+        if (t > nx + 1) return;
+        n = nz; g0 = a.p(l, t, s, 0); g1 = a.p(l, t, s, nz + 1); sn = a.p(l, t, s, nz); s1 = a.p(l, t, s, 1);
+    }
+    const float v0 = *g0, v1 = *g1, wn = *sn, w1 = *s1;
+    *g0 = 0.0f;
+    *g1 = 0.0f;
+    if (n == 1) {
+        *sn = wn + v0 + v1;
+    } else {
+        *sn = wn + v0;
+        *s1 = w1 + v1;
+    }
+}
+
+// reverse of k_closed (same grid): per pair, f1(m,G) = f2(l,G) and
+// f1(l,G) = f1(l,S) become f2^(l,G) += f1^(m,G), f1^(l,S) += f1^(l,G) with the
+// ghost adjoints zeroed.  The reflected directions m and the outgoing l are
+// disjoint sets and S is interior, so all loads can precede the stores.
+template <typename Acc>
+__global__ void __launch_bounds__(128) k_closed_adj(Acc f1, Acc f2, int axis, FacePairs lo, FacePairs hi) {
+    const int nx = f1.g.nx, ny = f1.g.ny, nz = f1.g.nz;
+    const int side = blockIdx.z;
+    const FacePairs& fp = side ? hi : lo;
+    const int a = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int b = blockIdx.y + 1;
+    int i, j, k, pi, pj, pk;
+    if (axis == 0) {
+        if (a > ny) return;
+        j = a; k = b; i = side ? nx + 1 : 0; pi = side ? nx : 1; pj = j; pk = k;
+    } else if (axis == 1) {
+        if (a > nx) return;
+        i = a; k = b; j = side ? ny + 1 : 0; pj = side ? ny : 1; pi = i; pk = k;
+    } else {
+        if (a > nx) return;
+        i = a; j = b; k = side ? nz + 1 : 0; pk = side ? nz : 1; pi = i; pj = j;
+    }
+    float wm[9], wl[9], a2[9], ws[9];
+    float* ps[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        if (q >= fp.n) break;
+        const int l = fp.l[q], m = fp.m[q];
+        const int si = (axis == 0) ? pi : pi - fp.cx[q];
+        const int sj = (axis == 1) ? pj : pj - fp.cy[q];
+        const int sk = (axis == 2) ? pk : pk - fp.cz[q];
+        ps[q] = f1.p(l, si, sj, sk);
+        wm[q] = *f1.p(m, i, j, k);
+        wl[q] = *f1.p(l, i, j, k);
+        a2[q] = *f2.p(l, i, j, k);
+        ws[q] = *ps[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        if (q >= fp.n) break;
+        const int l = fp.l[q], m = fp.m[q];
+        *f1.p(m, i, j, k) = 0.0f;
+        *f1.p(l, i, j, k) = 0.0f;
+        *f2.p(l, i, j, k) = a2[q] + wm[q];
+        *ps[q] = ws[q] + wl[q];
+    }
 }
 
 }  // namespace lbm

@@ -18,14 +18,14 @@ int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
         if (axis == 0) grd = dim3((ny + 2 + 127) / 128, nz + 2, nl);
         else if (axis == 1) grd = dim3((nx + 2 + 127) / 128, nz + 2, nl);
         else grd = dim3((nx + 2 + 127) / 128, ny + 2, nl);
-        k_periodic<AdjA><<<grd, 128, 0, s>>>(a1, axis, nl);
+        k_periodic_adj<AdjA><<<grd, 128, 0, s>>>(a1, axis, nl);
         c->launches++;
     };
     const int codes[3] = {c->p.ibnd, c->p.jbnd, c->p.kbnd};
     for (int a = 2; a >= 0; --a)
         if (codes[a] == 0) periodic(a);
     if (c->p.ibnd == 1) {
-        k_inflow_adj<Q, AdjA><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(a1, uvelh, c->p.rho0, c->cosd, c->sind);
+        k_inflow_adj<Q, AdjA><<<dim3((ny + 31) / 32, nz), 32, 0, s>>>(a1, uvelh, c->p.rho0, c->cosd, c->sind);
         c->launches++;
     }
     if (c->corners_on) {
@@ -42,7 +42,7 @@ int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
         if (!c->face_on[a]) continue;
         const int na = (a == 0) ? ny : nx;
         const int nb = (a == 2) ? ny : nz;
-        k_closed<AdjA><<<dim3((na + 127) / 128, nb, 2), 128, 0, s>>>(a1, a2, a, c->face[a][0], c->face[a][1], 1, 1);
+        k_closed_adj<AdjA><<<dim3((na + 127) / 128, nb, 2), 128, 0, s>>>(a1, a2, a, c->face[a][0], c->face[a][1]);
         c->launches++;
     }
     for (int a = 2; a >= 0; --a)
@@ -165,21 +165,22 @@ int lbm_state_adjoint_step(lbm_ctx* c, float* W, float* A, const void* P, int32_
     LBM_TRY(sadj_check(c, "state_adjoint_step"));
     const SoaGrid& g = c->sg;
     const int Q = c->p.nl;
-    const dim3 all((g.nx + 2 + 127) / 128, g.ny + 2, g.nz + 2), inner((g.nx + 127) / 128, g.ny, g.nz);
-    if (Q == 27) k_sadj_pull_t<27><<<all, 128, 0, c->stream>>>(W, A, g);
-    else k_sadj_pull_t<19><<<all, 128, 0, c->stream>>>(W, A, g);
+    const unsigned shell = (unsigned)((sadj_shell_cells(g) + 127) / 128);
+    const dim3 inner((g.nx + 127) / 128, g.ny, g.nz);
+    if (Q == 27) k_sadj_shell<27><<<shell, 128, 0, c->stream>>>(W, A, g);
+    else k_sadj_shell<19><<<shell, 128, 0, c->stream>>>(W, A, g);
     c->launches++;
-    LBM_LAUNCHED(c, "state adjoint: drift");
+    LBM_LAUNCHED(c, "state adjoint: shell");
     SoaAdjAcc a1{W, g}, a2{A, g};
     LBM_TRY(Q == 27 ? run_bc_adj<27>(c, a1, a2, uvelhat) : run_bc_adj<19>(c, a1, a2, uvelhat));
     const int wrap = (c->p.jbnd == 0) ? 1 : 0;
     const float* Pf = static_cast<const float*>(P);
     if (Q == 27) {
-        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
     } else {
-        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
     }
     c->launches++;
     LBM_LAUNCHED(c, "state adjoint: collision");

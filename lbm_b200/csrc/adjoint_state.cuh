@@ -12,6 +12,8 @@
 // pull is a shift by +c_l of each direction's block.
 #pragma once
 
+#include <algorithm>
+
 #include "adjoint.cuh"
 #include "state_kernels.cuh"
 
@@ -37,51 +39,98 @@ __device__ __forceinline__ bool interior(const SoaGrid& g, int i, int j, int k) 
     return i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
 }
 
-// drift adjoint: W(l, y) += A(l, y + c_l) for every cell y whose target y + c_l is
-// interior, and A(l, y + c_l) = 0.  Each interior element of A is read by exactly
-// one thread, which also clears it.  Grid: x over i = 0..nx+1, y = j, z = k.
-template <int Q>
-__global__ void __launch_bounds__(128) k_sadj_pull_t(float* __restrict__ W, float* __restrict__ A, SoaGrid g) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx + 1) return;
-    const long long o = g.off(i, j, k);
-    const long long plane = (long long)g.pitch * (g.ny + 2);
-    // all loads first, then the clears and accumulations: the compiler cannot tell
-    // that the directions' blocks do not overlap, so a per-direction
-    // load/clear/accumulate chain would run one memory round trip at a time
-    float v[Q];
-    bool in[Q];
-#pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        in[l] = interior(g, i + lat_cx(l), j + lat_cy(l), k + lat_cz(l));
-        v[l] = in[l] ? A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane]
-                     : 0.0f;
-    }
-    float w[Q];
-#pragma unroll
-    for (int l = 0; l < Q; ++l) w[l] = W[(long long)l * g.dstride + o];
-#pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        if (!in[l]) continue;
-        A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane] = 0.0f;
-        W[(long long)l * g.dstride + o] = w[l] + v[l];
-    }
+// the ghost shell and the interior cells next to it: the only cells whose
+// adjoint entries the boundary adjoint reads or writes
+__device__ __forceinline__ bool near_shell(const SoaGrid& g, int i, int j, int k) {
+    return i <= 1 || i >= g.nx || j <= 1 || j >= g.ny || k <= 1 || k >= g.nz;
 }
 
-// postcoll (+solids, +the macrovars of its input) adjoint at interior cells: W
-// holds the adjoint of the post-collision populations and receives that of the
-// pre-collision ones.  PULL: the forward input is pull(P) (P a copy of the
-// previous step's fused state buffer, offsets f - w, FP32); otherwise it is P
-// itself (the state as imported).  wrap: periodic j without stored ghost rows.
+// the k-th of the distinct values {0, 1, n, n+1} (count: min(4, n + 2))
+__device__ __forceinline__ int edge_value(int idx, int n) {
+    const int cnt = min(4, n + 2);
+    return idx < 2 ? idx : n + 2 - cnt + idx;
+}
+
+// Before the boundary adjoint.  (1) The drift transpose for ghost targets:
+// W(l, y) += A(l, y + c_l) for ghost cells y whose target y + c_l is interior.
+// (2) W(l, y) = 0 at the interior cells next to the shell: the interior of f2
+// is overwritten by the next step's collision, so its adjoint is zero before
+// the boundary adjoint accumulates into it.  Interior elements of A are read,
+// not cleared; the cell kernel reads each of the others exactly once.
+// A thread per cell of the two outer layers: first the whole rows (j, k) with
+// j or k in {0, 1, n, n+1} (coalesced), then the cells i in {0, 1, nx, nx+1}
+// of the other rows.
+template <int Q>
+__global__ void __launch_bounds__(128) k_sadj_shell(float* __restrict__ W, const float* __restrict__ A, SoaGrid g) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int ck = min(4, nz + 2), cj = min(4, ny + 2), cx = min(4, nx + 2);
+    const int kin = max(0, nz - 2), jin = max(0, ny - 2);
+    const long long full_rows = (long long)ck * (ny + 2) + (long long)cj * kin;
+    const long long nfull = full_rows * (nx + 2);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (t < nfull) {
+        const long long r = t / (nx + 2);
+        i = (int)(t - r * (nx + 2));
+        if (r < (long long)ck * (ny + 2)) {
+            k = edge_value((int)(r / (ny + 2)), nz);
+            j = (int)(r % (ny + 2));
+        } else {
+            const int q = (int)(r - (long long)ck * (ny + 2));
+            j = edge_value(q / kin, ny);
+            k = 2 + q % kin;
+        }
+    } else {
+        const long long u = t - nfull;
+        if (u >= (long long)jin * kin * cx) return;
+        const int r = (int)(u / cx);
+        i = edge_value((int)(u - (long long)r * cx), nx);
+        j = 2 + r % jin;
+        k = 2 + r / jin;
+    }
+    const long long o = g.off(i, j, k);
+    if (interior(g, i, j, k)) {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) W[(long long)l * g.dstride + o] = 0.0f;
+        return;
+    }
+    const long long plane = (long long)g.pitch * (g.ny + 2);
+    float v[Q], w[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        v[l] = interior(g, i + lat_cx(l), j + lat_cy(l), k + lat_cz(l))
+                   ? A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane]
+                   : 0.0f;
+        w[l] = W[(long long)l * g.dstride + o];
+    }
+#pragma unroll
+    for (int l = 0; l < Q; ++l) W[(long long)l * g.dstride + o] = w[l] + v[l];
+}
+
+// threads of k_sadj_shell
+inline long long sadj_shell_cells(const SoaGrid& g) {
+    const long long ck = std::min(4, g.nz + 2), cj = std::min(4, g.ny + 2), cx = std::min(4, g.nx + 2);
+    const long long kin = std::max(0, g.nz - 2), jin = std::max(0, g.ny - 2);
+    return (ck * (g.ny + 2) + cj * kin) * (g.nx + 2) + jin * kin * cx;
+}
+
+// One reverse step at the interior cells: the drift transpose for interior
+// targets, gh(l, y) = A(l, y + c_l) (+ W(l, y), the boundary adjoint's
+// contributions, next to the shell), then the postcoll (+solids, +the
+// macrovars of its input) adjoint; W receives the adjoint of the pre-collision
+// populations.  PULL: the forward input is pull(P) (P a copy of the previous
+// step's fused state buffer, offsets f - w, FP32); otherwise it is P itself
+// (the state as imported).  wrap: periodic j without stored ghost rows.
 template <int Q, bool PULL>
-__global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const float* __restrict__ P, SoaGrid g,
-                                                   int wrap, const uint8_t* __restrict__ solid, CollideParams cp,
+__global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const float* __restrict__ A,
+                                                   const float* __restrict__ P, SoaGrid g, int wrap,
+                                                   const uint8_t* __restrict__ solid, CollideParams cp,
                                                    const float* __restrict__ abl) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
     if (i > g.nx) return;
     const long long o = g.off(i, j, k);
+    const long long plane = (long long)g.pitch * (g.ny + 2);
     float fp[Q], gh[Q], fh[Q];
     if (PULL) {
         PullMacro<Q, float, 0>::run(fp, P, g, o, j, wrap != 0);
@@ -90,7 +139,14 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
         for (int l = 0; l < Q; ++l) fp[l] = P[(long long)l * g.dstride + o];
     }
 #pragma unroll
-    for (int l = 0; l < Q; ++l) gh[l] = W[(long long)l * g.dstride + o];
+    for (int l = 0; l < Q; ++l)
+        gh[l] = A[(long long)l * g.dstride + o + lat_cx(l) + (long long)lat_cy(l) * g.pitch + lat_cz(l) * plane];
+    if (near_shell(g, i, j, k)) {
+#pragma unroll
+        for (int l = 0; l < Q; ++l)
+            gh[l] = (interior(g, i + lat_cx(l), j + lat_cy(l), k + lat_cz(l)) ? gh[l] : 0.0f) +
+                    W[(long long)l * g.dstride + o];
+    }
     if (solid && solid[((long long)(k - 1) * g.ny + (j - 1)) * g.nx + (i - 1)]) {
 #pragma unroll
         for (int l = 1; l + 1 < Q; l += 2) {

@@ -2,6 +2,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,7 +49,8 @@ struct lbm_ctx {
     bool corners_on = false;
     float cosd = 1.f, sind = 0.f;
     // fused state
-    void* buf[2] = {nullptr, nullptr};
+    void* buf[2] = {nullptr, nullptr};   // the two buffers a step reads and writes
+    void* own[2] = {nullptr, nullptr};   // the context's allocations (buf may point at a caller's, lbm_step_to)
     size_t elem = 4;
     int cur = 0;
     int state = ST_NONE;
@@ -501,6 +503,28 @@ int step_one(lbm_ctx* c) {
     return LBM_OK;
 }
 
+// dst takes the place of the buffer the next step would overwrite: it receives
+// that buffer's ghost shell (the boundaries read ghost values of two steps before)
+void take_dst(lbm_ctx* c, void* dst) {
+    void* prev = c->buf[1 - c->cur];
+    if (prev != dst) {
+        const dim3 grd((unsigned)((ghost_cells(c->sg) + 127) / 128), (unsigned)c->p.nl);
+        if (c->elem == 2)
+            k_copy_ghosts<uint16_t><<<grd, 128, 0, c->stream>>>((uint16_t*)dst, (const uint16_t*)prev, c->sg);
+        else
+            k_copy_ghosts<uint32_t><<<grd, 128, 0, c->stream>>>((uint32_t*)dst, (const uint32_t*)prev, c->sg);
+        c->launches++;
+    }
+    c->buf[1 - c->cur] = dst;
+}
+
+// the next step writes into one of the context's own buffers (not the one it reads)
+void own_dst(lbm_ctx* c) {
+    const int n = 1 - c->cur;
+    if ((c->buf[n] == c->own[0] || c->buf[n] == c->own[1]) && c->buf[n] != c->buf[c->cur]) return;
+    take_dst(c, (c->buf[c->cur] == c->own[n]) ? c->own[1 - n] : c->own[n]);
+}
+
 int step_dispatch(lbm_ctx* c) {
     const bool h = c->p.storage == LBM_STORE_F16;
     if (c->p.nl == 27) return h ? step_one<27, __half>(c) : step_one<27, float>(c);
@@ -606,8 +630,9 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     // + 1 KiB: the bulk copies of k_step_tma read up to ~100 elements past the last row
     const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem + 1024;
     for (int b = 0; b < 2 && rc == LBM_OK; ++b) {
-        chk(cudaMalloc(&c->buf[b], nbuf), "cudaMalloc(state)");
-        if (rc == LBM_OK) chk(cudaMemset(c->buf[b], 0, nbuf), "cudaMemset(state)");
+        chk(cudaMalloc(&c->own[b], nbuf), "cudaMalloc(state)");
+        if (rc == LBM_OK) chk(cudaMemset(c->own[b], 0, nbuf), "cudaMemset(state)");
+        c->buf[b] = c->own[b];
     }
     const size_t g = (size_t)c->rg.ncell();
     chk(cudaMalloc(&c->d_macro, 4 * g * sizeof(float)), "cudaMalloc(macro)");
@@ -639,7 +664,7 @@ int lbm_destroy(lbm_ctx* c) {
     if (!c) return LBM_ERR_ARG;
     cudaStreamSynchronize(c->stream);
     for (cudaEvent_t e : c->ev) cudaEventDestroy(e);
-    for (int b = 0; b < 2; ++b) cudaFree(c->buf[b]);
+    for (int b = 0; b < 2; ++b) cudaFree(c->own[b]);
     cudaFree(c->d_macro);
     cudaFree(c->d_solid);
     cudaFree(c->d_turb);
@@ -841,6 +866,8 @@ int lbm_state_import(lbm_ctx* c, const float* f1, const float* f2, const float* 
                      const float* w, int32_t it) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f1); NEED(c, f2); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    c->buf[0] = c->own[0];
+    c->buf[1] = c->own[1];
     DISPATCH_QS(c, launch_import, c, f1, 0);
     DISPATCH_QS(c, launch_import, c, f2, 1);
     const size_t g = (size_t)c->rg.ncell() * sizeof(float);
@@ -952,8 +979,30 @@ int lbm_step(lbm_ctx* c, int32_t nsteps) {
     if (!c) return LBM_ERR_ARG;
     if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "step: no state imported");
     if (nsteps < 0) return fail(c, LBM_ERR_ARG, "step: nsteps < 0");
-    for (int s = 0; s < nsteps; ++s) LBM_TRY(step_dispatch(c));
+    for (int s = 0; s < nsteps; ++s) {
+        own_dst(c);
+        LBM_LAUNCHED(c, "step: ghost shell");
+        LBM_TRY(step_dispatch(c));
+    }
     return LBM_OK;
+}
+
+int lbm_step_to(lbm_ctx* c, void* dst) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, dst);
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "step_to: no state imported");
+    if (reinterpret_cast<uintptr_t>(dst) % 256 != 0) return fail(c, LBM_ERR_ARG, "step_to: dst not 256-byte aligned");
+    if (dst == c->buf[c->cur] || dst == c->own[0] || dst == c->own[1])
+        return fail(c, LBM_ERR_ARG, "step_to: dst is one of the context's buffers");
+    if (c->state == ST_PRE) {
+        // the first step after an import collides in place: step, then copy
+        own_dst(c);
+        LBM_TRY(step_dispatch(c));
+        return lbm_state_copy(c, dst);
+    }
+    take_dst(c, dst);
+    LBM_LAUNCHED(c, "step_to: ghost shell");
+    return step_dispatch(c);
 }
 
 int lbm_step_host(lbm_ctx* c, int32_t nsteps, const float* uvel_host, int32_t* status_host) {
@@ -964,6 +1013,7 @@ int lbm_step_host(lbm_ctx* c, int32_t nsteps, const float* uvel_host, int32_t* s
         if (uvel_host)
             LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_uvel, uvel_host, (size_t)c->p.nz * sizeof(float),
                                                   cudaMemcpyHostToDevice, c->stream), "step_host uvel"));
+        own_dst(c);
         LBM_TRY(step_dispatch(c));
     }
     if (status_host) {

@@ -139,6 +139,10 @@ int ens_align(lbm_ensemble* e, int* used) {
         lbm_ctx* c = e->m[k];
         if (c->state == ST_NONE) return efail(e, LBM_ERR_STATE, "member %d: no state imported", (int)k);
         if (c->force) return efail(e, LBM_ERR_UNSUPPORTED, "member %d: the ensemble kernels take no external forcing", (int)k);
+        if (c->buf[c->cur] != c->own[0] && c->buf[c->cur] != c->own[1])
+            return efail(e, LBM_ERR_STATE, "member %d: its state is in a caller's buffer (lbm_step_to); import it again",
+                         (int)k);
+        own_dst(c);
         if (c->state == ST_PRE) {
             LBM_TRY(emember(e, (int)k, step_dispatch(c)));
             pre = true;

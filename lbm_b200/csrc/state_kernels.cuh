@@ -233,6 +233,43 @@ __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a,
     bc_fold_block<Q, S>(f1, f2, a, nface_blocks, blockIdx.x);
 }
 
+// Copy every ghost entry (all directions) of one state buffer to another: the
+// ghost cells a step leaves alone, or fills from the buffer's own earlier
+// contents (the two-timestep bounce-back), as the buffer it replaces held them.
+// Threads over the ghost cells: whole rows with k in {0, nz+1} or j in {0, ny+1},
+// then i in {0, nx+1} of the other rows; blockIdx.y = direction.
+template <typename T>
+__global__ void __launch_bounds__(128) k_copy_ghosts(T* __restrict__ dst, const T* __restrict__ src, SoaGrid g) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long nfull = (2LL * (ny + 2) + 2LL * nz) * (nx + 2);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (t < nfull) {
+        const long long r = t / (nx + 2);
+        i = (int)(t - r * (nx + 2));
+        if (r < 2LL * (ny + 2)) {
+            k = (r < ny + 2) ? 0 : nz + 1;
+            j = (int)(r % (ny + 2));
+        } else {
+            const int q = (int)(r - 2LL * (ny + 2));
+            j = (q < nz) ? 0 : ny + 1;
+            k = 1 + q % nz;
+        }
+    } else {
+        const long long u = t - nfull;
+        if (u >= 2LL * ny * nz) return;
+        i = (u & 1) ? nx + 1 : 0;
+        const long long r = u >> 1;
+        j = 1 + (int)(r % ny);
+        k = 1 + (int)(r / ny);
+    }
+    const long long o = (long long)blockIdx.y * g.dstride + g.off(i, j, k);
+    dst[o] = src[o];
+}
+inline long long ghost_cells(const SoaGrid& g) {
+    return (2LL * (g.ny + 2) + 2LL * g.nz) * (g.nx + 2) + 2LL * g.ny * g.nz;
+}
+
 // Folded configuration: copy the x-ghost columns of a buffer whose rows hold
 // every direction (after an import or a step with the general boundary
 // kernels) into its compact array.  One thread per element of xg.

@@ -319,6 +319,29 @@ def test_state_layout_sweep_matches_fp64_finite_differences(nl):
     fb.close()
 
 
+@pytest.mark.parametrize("codes", [(11, 22, 12), (0, 0, 0), (1, 11, 22), (0, 12, 0)])
+@pytest.mark.parametrize("nl", [19, 27])
+def test_state_layout_sweep_matches_per_call_sweep_for_boundary_codes(codes, nl):
+    """Closed faces, edges and corners, periodic axes and inflow: the boundary
+    adjoint reaches the cells next to every face."""
+    ib, jb, kb = codes
+    wl = CASE.with_(nl=nl, ibnd=ib, jbnd=jb, kbnd=kb, steps=8)
+    pb, f1, f2, uvel = problem(wl, 3)
+    fb = fused_problem(wl, 3, None)
+    rng = np.random.default_rng(7)
+    uhat = cuda(rng.standard_normal((len(fb.probes), 3)))
+    fb.forward(f1, f2, uvel)
+    gf, gu = (host(t) for t in fb.backward(uhat))
+    pb.forward(f1, f2, uvel)
+    rf, ru = (host(t) for t in pb.backward(uhat))
+    assert np.abs(rf).max() > 0
+    assert np.abs(gf - rf).max() <= 1e-4 * np.abs(rf).max(), codes
+    if ib == 1:
+        assert np.abs(gu - ru).max() <= 1e-4 * np.abs(ru).max()
+    pb.close()
+    fb.close()
+
+
 def test_state_layout_sweep_refuses_unsupported_states():
     from lbm_b200 import LbmError, Params
     from lbm_b200.adjoint import FusedProbeProblem
