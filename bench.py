@@ -572,9 +572,9 @@ def adjoint_bench(a):
                                    "reverse_over_forward": round(ts_bwd / ts_fwd, 3),
                                    "reverse_over_fused_forward": round(ts_bwd / t_fused, 3),
                                    "gradient_vs_per_call_sweep": agree,
-                                   "how": "forward by the fused step with checkpoints (reference-layout export); "
-                                          "reverse replays each segment with the fused step and runs "
-                                          "lbm_state_adjoint_step"},
+                                   "how": "forward by the fused step with a device snapshot every 10 steps "
+                                          "(lbm_state_snapshot); reverse restores each segment, replays it "
+                                          "into per-step buffers (lbm_step_to) and runs lbm_state_adjoint_step"},
             "forward_mlups": round(cells * wl.steps / (t_fwd * 1e-3) / 1e6, 1),
             "loss": loss, "grad_norm": {"f1": gnorm_f, "uvel": gnorm_u},
             "gradient_check": "tests/test_gpu_adjoint.py: central FP64 differences, 8 seeded directions, rel <= 1e-4",

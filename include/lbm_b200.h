@@ -172,6 +172,17 @@ int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
 int lbm_set_forcing(lbm_ctx* ctx, const float* external_forcing);
 /* advance nsteps time steps */
 int lbm_step(lbm_ctx* ctx, int32_t nsteps);
+/* Snapshots of a stepped state in device memory: everything a context needs to
+ * resume from that step (its state buffer, the ghost shell the next boundaries
+ * read, the compact x-ghost columns and the step number).  A snapshot restores
+ * into any context created with the same parameters.  lbm_state_snapshot needs
+ * a state that has been stepped at least once (after an import the caller
+ * holds f1, f2 already); dst and src are 256-byte aligned device memory of
+ * lbm_state_snapshot_bytes bytes.  The first lbm_state_bytes bytes of a
+ * snapshot are the state buffer (as lbm_state_copy). */
+int lbm_state_snapshot_bytes(lbm_ctx* ctx, int64_t* bytes);
+int lbm_state_snapshot(lbm_ctx* ctx, void* dst);
+int lbm_state_restore(lbm_ctx* ctx, const void* src);
 /* one time step whose result (the state buffer lbm_state_copy would give) is
  * written to dst, device memory of lbm_state_bytes bytes, 256-byte aligned, that
  * the caller owns, instead of to the context's other buffer.  The context reads

@@ -154,6 +154,19 @@ module lbm_b200_iface
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, dst
       end function
+      integer(c_int) function lbm_state_snapshot_bytes(ctx, bytes) bind(C, name="lbm_state_snapshot_bytes")
+         import :: c_ptr, c_int, c_int64_t
+         type(c_ptr), value     :: ctx
+         integer(c_int64_t)     :: bytes
+      end function
+      integer(c_int) function lbm_state_snapshot(ctx, dst) bind(C, name="lbm_state_snapshot")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, dst
+      end function
+      integer(c_int) function lbm_state_restore(ctx, src) bind(C, name="lbm_state_restore")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, src
+      end function
       integer(c_int) function lbm_step_host(ctx, nsteps, uvel_host, status) bind(C, name="lbm_step_host")
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value        :: ctx, uvel_host

@@ -78,6 +78,9 @@ SIGNATURES = {
     "lbm_forcings_apply": [P, P, P, P, P, P, P],
     "lbm_step": [P, I],
     "lbm_step_to": [P, P],
+    "lbm_state_snapshot_bytes": [P, P],
+    "lbm_state_snapshot": [P, P],
+    "lbm_state_restore": [P, P],
     "lbm_set_kernel": [P, I],
     "lbm_step_host": [P, I, P, ctypes.POINTER(ctypes.c_int32)],
     "lbm_get_step": [P, ctypes.POINTER(ctypes.c_int32)],

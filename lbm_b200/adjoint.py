@@ -135,10 +135,11 @@ def initial_state(lbm: Lbm, rho, u, v, w, uvel):
 class FusedProbeProblem:
     """The probe-misfit problem of :class:`ProbeProblem` with the forward run made
     by the fused step (the library's default kernels) and the reverse sweep in
-    the state layout (``lbm_state_adjoint_*``).  Checkpoints are the
-    reference-layout (f1, f2) every ``checkpoint`` steps; each segment is
-    replayed from its checkpoint by importing it again (rho, u from macrovars),
-    each step writing its state buffer into an array of its own (lbm_step_to)."""
+    the state layout (``lbm_state_adjoint_*``).  Checkpoints are the initial
+    (f1, f2) and, every ``checkpoint`` steps after it, a device snapshot of the
+    fused state (``lbm_state_snapshot``).  Each segment is replayed from its
+    checkpoint, each step writing its state buffer into an array of its own
+    (``lbm_step_to``)."""
 
     def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
         if params.storage != "f32":
@@ -170,10 +171,7 @@ class FusedProbeProblem:
         self._import(f1, f2)
         for n in range(self.nsteps):
             if keep and n % self.K == 0:
-                a, b = (f1.clone(), f2.clone()) if n == 0 else (L.empty_f(), L.empty_f())
-                if n > 0:
-                    L.state_export(a, b)
-                self.ckpt[n] = (a, b)
+                self.ckpt[n] = (f1.clone(), f2.clone()) if n == 0 else L.snapshot()
             L.step(1)
         R = [L.empty_s() for _ in range(4)]
         L.get_macro(*R)
@@ -185,9 +183,14 @@ class FusedProbeProblem:
         uvel_h = torch.zeros(self.p.nz, dtype=torch.float32, device="cuda")
         for s in sorted(self.ckpt, reverse=True):
             e = min(s + self.K, self.nsteps)
-            self._import(*self.ckpt[s])
-            D = L.state_scratch()
-            L.state_copy(D)                   # the imported f1: input of step s
+            if s == 0:
+                self._import(*self.ckpt[s])
+                first = L.state_scratch()
+                L.state_copy(first)           # the imported f1: input of step 0
+            else:
+                first = self.ckpt[s]          # the state after step s - 1, which step s pulls from
+                L.restore(first)
+                L.set_inflow(self.uvel)
             P = []
             for _ in range(s, e):
                 P.append(L.state_scratch())
@@ -195,10 +198,10 @@ class FusedProbeProblem:
             if e == self.nsteps:
                 L.state_adjoint_seed(A, P[-1], self.probes_dev, uhat_probes.float())
             for n in range(e - 1, s - 1, -1):
-                src = P[n - s - 1] if n > s else D
-                L.state_adjoint_step(W, A, src, n > s, uvel_h)
+                src = P[n - s - 1] if n > s else first
+                L.state_adjoint_step(W, A, src, n > s or s > 0, uvel_h)
                 W, A = A, W                   # A: adjoint of f1 before step n, W: of f2
-            del P, D
+            del P, first
         g = L.empty_f()
         L.state_adjoint_export(g, A)
         return g, uvel_h

@@ -315,6 +315,22 @@ class Lbm:
     def step(self, nsteps=1):
         self._call("lbm_step", ctypes.c_int32(nsteps))
 
+    def snapshot_bytes(self) -> int:
+        n = ctypes.c_int64(0)
+        self._call("lbm_state_snapshot_bytes", ctypes.byref(n))
+        return int(n.value)
+
+    def snapshot(self, dst=None):
+        """Device snapshot of the stepped state (allocated when ``dst`` is None)."""
+        if dst is None:
+            dst = torch.empty((self.snapshot_bytes() + 3) // 4, dtype=torch.float32, device="cuda")
+        self._call("lbm_state_snapshot", _ptr(dst))
+        return dst
+
+    def restore(self, src):
+        """Resume from a snapshot (same parameters)."""
+        self._call("lbm_state_restore", _ptr(src))
+
     def step_to(self, dst):
         """One step whose state buffer is written to ``dst`` (a :meth:`state_scratch`
         tensor, kept alive by the caller until two more steps or an import)."""

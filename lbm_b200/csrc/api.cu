@@ -1005,6 +1005,108 @@ int lbm_step_to(lbm_ctx* c, void* dst) {
     return step_dispatch(c);
 }
 
+// ---- snapshots: a stepped state kept in device memory and resumed later -------
+// Layout: the current buffer (as lbm_state_copy), the ghost shell of the other
+// buffer (packed, k_pack_ghosts), the x-ghost columns of both buffers (folded
+// configuration) and a header.  Each part starts on a 256-byte boundary.
+struct SnapLayout {
+    size_t buf, shell, xg, head, total;
+};
+struct SnapHead {
+    int32_t magic, it, nx, ny, nz, nl, storage, fold;
+};
+static const int32_t kSnapMagic = 0x4c424d53;   // "LBMS"
+
+static SnapLayout snap_layout(const lbm_ctx* c) {
+    auto up = [](size_t n) { return (n + 255) / 256 * 256; };
+    SnapLayout L;
+    L.buf = up((size_t)c->p.nl * c->sg.dstride * c->elem + 1024);
+    L.shell = up((size_t)c->p.nl * ghost_cells(c->sg) * c->elem);
+    L.xg = c->fold ? up((size_t)2 * c->p.nl * c->p.ny * c->p.nz * c->elem) : 0;
+    L.head = 256;
+    L.total = L.buf + L.shell + 2 * L.xg + L.head;
+    return L;
+}
+
+static void pack_ghosts(lbm_ctx* c, void* packed, void* buf, bool unpack) {
+    const long long n = ghost_cells(c->sg);
+    const dim3 grd((unsigned)((n + 127) / 128), (unsigned)c->p.nl);
+    if (c->elem == 2) {
+        if (unpack) k_pack_ghosts<uint16_t, true><<<grd, 128, 0, c->stream>>>((uint16_t*)packed, (uint16_t*)buf, c->sg, n);
+        else k_pack_ghosts<uint16_t, false><<<grd, 128, 0, c->stream>>>((uint16_t*)packed, (uint16_t*)buf, c->sg, n);
+    } else {
+        if (unpack) k_pack_ghosts<uint32_t, true><<<grd, 128, 0, c->stream>>>((uint32_t*)packed, (uint32_t*)buf, c->sg, n);
+        else k_pack_ghosts<uint32_t, false><<<grd, 128, 0, c->stream>>>((uint32_t*)packed, (uint32_t*)buf, c->sg, n);
+    }
+    c->launches++;
+}
+
+int lbm_state_snapshot_bytes(lbm_ctx* c, int64_t* bytes) {
+    if (!c || !bytes) return LBM_ERR_ARG;
+    *bytes = (int64_t)snap_layout(c).total;
+    return LBM_OK;
+}
+
+int lbm_state_snapshot(lbm_ctx* c, void* dst) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, dst);
+    if (c->state != ST_POST)
+        return fail(c, LBM_ERR_STATE, "state_snapshot: no stepped state (after an import, keep its f1, f2 instead)");
+    if (reinterpret_cast<uintptr_t>(dst) % 256 != 0) return fail(c, LBM_ERR_ARG, "state_snapshot: dst not 256-byte aligned");
+    const SnapLayout L = snap_layout(c);
+    char* d = static_cast<char*>(dst);
+    const size_t nbuf = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(d, c->buf[c->cur], nbuf, cudaMemcpyDeviceToDevice, c->stream), "snapshot"));
+    pack_ghosts(c, d + L.buf, c->buf[1 - c->cur], false);
+    if (c->fold) {
+        const size_t nxg = (size_t)2 * c->p.nl * c->p.ny * c->p.nz * c->elem;
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(d + L.buf + L.shell, c->d_xg[c->cur], nxg, cudaMemcpyDeviceToDevice,
+                                              c->stream), "snapshot"));
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(d + L.buf + L.shell + L.xg, c->d_xg[1 - c->cur], nxg,
+                                              cudaMemcpyDeviceToDevice, c->stream), "snapshot"));
+    }
+    const SnapHead h{kSnapMagic, c->it, c->p.nx, c->p.ny, c->p.nz, c->p.nl, c->p.storage, c->fold ? 1 : 0};
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(d + L.buf + L.shell + 2 * L.xg, &h, sizeof(h), cudaMemcpyHostToDevice,
+                                          c->stream), "snapshot"));
+    LBM_LAUNCHED(c, "snapshot");
+    return LBM_OK;
+}
+
+int lbm_state_restore(lbm_ctx* c, const void* src) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, src);
+    if (reinterpret_cast<uintptr_t>(src) % 256 != 0) return fail(c, LBM_ERR_ARG, "state_restore: src not 256-byte aligned");
+    const SnapLayout L = snap_layout(c);
+    const char* s = static_cast<const char*>(src);
+    SnapHead h;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(&h, s + L.buf + L.shell + 2 * L.xg, sizeof(h), cudaMemcpyDeviceToHost,
+                                          c->stream), "restore"));
+    LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "restore"));
+    if (h.magic != kSnapMagic || h.nx != c->p.nx || h.ny != c->p.ny || h.nz != c->p.nz || h.nl != c->p.nl ||
+        h.storage != c->p.storage || h.fold != (c->fold ? 1 : 0))
+        return fail(c, LBM_ERR_ARG, "state_restore: not a snapshot of a context with these parameters");
+    c->buf[0] = c->own[0];
+    c->buf[1] = c->own[1];
+    const size_t nbuf = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->buf[0], s, nbuf, cudaMemcpyDeviceToDevice, c->stream), "restore"));
+    pack_ghosts(c, const_cast<char*>(s) + L.buf, c->buf[1], true);
+    if (c->fold) {
+        const size_t nxg = (size_t)2 * c->p.nl * c->p.ny * c->p.nz * c->elem;
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_xg[0], s + L.buf + L.shell, nxg, cudaMemcpyDeviceToDevice, c->stream),
+                           "restore"));
+        LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_xg[1], s + L.buf + L.shell + L.xg, nxg, cudaMemcpyDeviceToDevice,
+                                              c->stream), "restore"));
+    }
+    const int nxt = h.it + 1;
+    LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->d_it, &nxt, sizeof(int), cudaMemcpyHostToDevice, c->stream), "restore"));
+    LBM_TRY(cuda_check(c, cudaStreamSynchronize(c->stream), "restore"));
+    LBM_LAUNCHED(c, "restore");
+    c->cur = 0;
+    c->it = h.it;
+    c->state = ST_POST;
+    return LBM_OK;
+}
+
 int lbm_step_host(lbm_ctx* c, int32_t nsteps, const float* uvel_host, int32_t* status_host) {
     if (!c) return LBM_ERR_ARG;
     if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "step_host: no state imported");

@@ -233,17 +233,12 @@ __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a,
     bc_fold_block<Q, S>(f1, f2, a, nface_blocks, blockIdx.x);
 }
 
-// Copy every ghost entry (all directions) of one state buffer to another: the
-// ghost cells a step leaves alone, or fills from the buffer's own earlier
-// contents (the two-timestep bounce-back), as the buffer it replaces held them.
-// Threads over the ghost cells: whole rows with k in {0, nz+1} or j in {0, ny+1},
-// then i in {0, nx+1} of the other rows; blockIdx.y = direction.
-template <typename T>
-__global__ void __launch_bounds__(128) k_copy_ghosts(T* __restrict__ dst, const T* __restrict__ src, SoaGrid g) {
+// The ghost cells of a state buffer, numbered t = 0 .. ghost_cells(g) - 1: whole
+// rows with k in {0, nz+1} or j in {0, ny+1}, then i in {0, nx+1} of the other
+// rows.  Returns false past the last one.
+__device__ __forceinline__ bool ghost_cell(const SoaGrid& g, long long t, int& i, int& j, int& k) {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long nfull = (2LL * (ny + 2) + 2LL * nz) * (nx + 2);
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    int i, j, k;
     if (t < nfull) {
         const long long r = t / (nx + 2);
         i = (int)(t - r * (nx + 2));
@@ -255,19 +250,43 @@ __global__ void __launch_bounds__(128) k_copy_ghosts(T* __restrict__ dst, const 
             j = (q < nz) ? 0 : ny + 1;
             k = 1 + q % nz;
         }
-    } else {
-        const long long u = t - nfull;
-        if (u >= 2LL * ny * nz) return;
-        i = (u & 1) ? nx + 1 : 0;
-        const long long r = u >> 1;
-        j = 1 + (int)(r % ny);
-        k = 1 + (int)(r / ny);
+        return true;
     }
-    const long long o = (long long)blockIdx.y * g.dstride + g.off(i, j, k);
-    dst[o] = src[o];
+    const long long u = t - nfull;
+    if (u >= 2LL * ny * nz) return false;
+    i = (u & 1) ? nx + 1 : 0;
+    const long long r = u >> 1;
+    j = 1 + (int)(r % ny);
+    k = 1 + (int)(r / ny);
+    return true;
 }
 inline long long ghost_cells(const SoaGrid& g) {
     return (2LL * (g.ny + 2) + 2LL * g.nz) * (g.nx + 2) + 2LL * g.ny * g.nz;
+}
+
+// Copy every ghost entry (all directions) of one state buffer to another: the
+// ghost cells a step leaves alone, or fills from the buffer's own earlier
+// contents (the two-timestep bounce-back), as the buffer it replaces held them.
+// A thread per ghost cell, blockIdx.y = direction.
+template <typename T>
+__global__ void __launch_bounds__(128) k_copy_ghosts(T* __restrict__ dst, const T* __restrict__ src, SoaGrid g) {
+    int i, j, k;
+    if (!ghost_cell(g, (long long)blockIdx.x * blockDim.x + threadIdx.x, i, j, k)) return;
+    const long long o = (long long)blockIdx.y * g.dstride + g.off(i, j, k);
+    dst[o] = src[o];
+}
+
+// The ghost shell of a state buffer to or from a compact array
+// packed[l][t] (t: ghost_cell numbering).  UNPACK: packed -> buffer.
+template <typename T, bool UNPACK>
+__global__ void __launch_bounds__(128) k_pack_ghosts(T* packed, T* buf, SoaGrid g, long long ncells) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (!ghost_cell(g, t, i, j, k)) return;
+    const long long o = (long long)blockIdx.y * g.dstride + g.off(i, j, k);
+    const long long q = (long long)blockIdx.y * ncells + t;
+    if (UNPACK) buf[o] = packed[q];
+    else packed[q] = buf[o];
 }
 
 // Folded configuration: copy the x-ghost columns of a buffer whose rows hold
