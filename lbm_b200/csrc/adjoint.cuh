@@ -67,54 +67,77 @@ __device__ __forceinline__ void collide_adj(const float (&fp)[Q], const float (&
     const float vz = axz * ux + ayz * uy + azz * uz;
 
     // ---- reverse (C0 = A0 - 1.5 K tr with A0 = (rho - 1) - 1.5 rho |u|^2 enter only through their adjoints) ----
+    // Emission per opposite pair (l, l+1): f(l) = E + O, f(l+1) = E - O with
+    //   E / w = C0 + R45 cu^2 + K45 cac,  O / w = cu (D0 + R45o cu^2 + K135 cac) - K9 cau
+    // (cu = c.u, cac = c.a.c, cau = c.a.u).  Over the pairs, sum Eh phi(c) =
+    // sum_l g_l phi(c_l) for even phi and sum Oh psi(c) = sum_l g_l psi(c_l) for
+    // odd psi, g_l = w_l gh_l, so every adjoint sum of the emission is a
+    // contraction of the moments Gi = sum g c_i, Gij = sum g c_i c_j and
+    // Gijk = sum g c_i c_j c_k (Giii = Gi since c_i^3 = c_i on these lattices).
     float C0h = lat_w<Q>(0) * gh[0];
-    float R45h = 0.f, R45oh = 0.f, K45h = 0.f, K135h = 0.f, K9h = 0.f, D0h = 0.f;
-    float axxh = 0.f, ayyh = 0.f, azzh = 0.f, axyh = 0.f, axzh = 0.f, ayzh = 0.f;
-    float vxh = 0.f, vyh = 0.f, vzh = 0.f;
+    float Gx = 0.f, Gy = 0.f, Gz = 0.f;
+    float Gxx = 0.f, Gyy = 0.f, Gzz = 0.f, Gxy = 0.f, Gxz = 0.f, Gyz = 0.f;
+    float Gxxy = 0.f, Gxxz = 0.f, Gxyy = 0.f, Gyyz = 0.f, Gxzz = 0.f, Gyzz = 0.f, Gxyz = 0.f;
 #pragma unroll
     for (int l = 1; l < Q; l += 2) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
         const float w = lat_w<Q>(l);
-        const float cu = cdot(cx, cy, cz, ux, uy, uz);
-        float cac = 0.f;
-        macc(cac, cx * cx, axx);
-        macc(cac, cy * cy, ayy);
-        macc(cac, cz * cz, azz);
-        macc(cac, cx * cy, 2.0f * axy);   // macc takes coefficients -1, 0, 1
-        macc(cac, cx * cz, 2.0f * axz);
-        macc(cac, cy * cz, 2.0f * ayz);
-        const float cau = cdot(cx, cy, cz, vx, vy, vz);
-        const float cu2 = cu * cu;
-        const float Eh = w * (gh[l] + gh[l + 1]);   // f(l) = E + O, f(opposite) = E - O
+        const float Eh = w * (gh[l] + gh[l + 1]);
         const float Oh = w * (gh[l] - gh[l + 1]);
-        const float inner = D0 + R45o * cu2 + K135 * cac;
-        // E / w = C0 + R45 cu^2 + K45 cac
         C0h += Eh;
-        R45h += Eh * cu2;
-        K45h += Eh * cac;
-        float cuh = Eh * R45 * 2.0f * cu;
-        float cach = Eh * K45;
-        // O / w = cu (D0 + R45o cu^2 + K135 cac) - K9 cau
-        cuh += Oh * (inner + 2.0f * R45o * cu2);
-        D0h += Oh * cu;
-        R45oh += Oh * cu * cu2;
-        K135h += Oh * cu * cac;
-        cach += Oh * cu * K135;
-        K9h -= Oh * cau;
-        const float cauh = -Oh * K9;
-        macc(uxh, cx, cuh);
-        macc(uyh, cy, cuh);
-        macc(uzh, cz, cuh);
-        macc(axxh, cx * cx, cach);
-        macc(ayyh, cy * cy, cach);
-        macc(azzh, cz * cz, cach);
-        macc(axyh, cx * cy, 2.0f * cach);
-        macc(axzh, cx * cz, 2.0f * cach);
-        macc(ayzh, cy * cz, 2.0f * cach);
-        macc(vxh, cx, cauh);
-        macc(vyh, cy, cauh);
-        macc(vzh, cz, cauh);
+        macc(Gx, cx, Oh);
+        macc(Gy, cy, Oh);
+        macc(Gz, cz, Oh);
+        macc(Gxx, cx * cx, Eh);
+        macc(Gyy, cy * cy, Eh);
+        macc(Gzz, cz * cz, Eh);
+        macc(Gxy, cx * cy, Eh);
+        macc(Gxz, cx * cz, Eh);
+        macc(Gyz, cy * cz, Eh);
+        macc(Gxxy, cx * cx * cy, Oh);
+        macc(Gxxz, cx * cx * cz, Oh);
+        macc(Gxyy, cx * cy * cy, Oh);
+        macc(Gyyz, cy * cy * cz, Oh);
+        macc(Gxzz, cx * cz * cz, Oh);
+        macc(Gyzz, cy * cz * cz, Oh);
+        macc(Gxyz, cx * cy * cz, Oh);
     }
+    // Gu_i = Gij u_j; Tu_ij = Gijk u_k; Tuu_i = Tu_ij u_j; Ta_i = Gijk a_jk
+    const float Gux = Gxx * ux + Gxy * uy + Gxz * uz;
+    const float Guy = Gxy * ux + Gyy * uy + Gyz * uz;
+    const float Guz = Gxz * ux + Gyz * uy + Gzz * uz;
+    const float Tuxx = Gx * ux + Gxxy * uy + Gxxz * uz;
+    const float Tuyy = Gxyy * ux + Gy * uy + Gyyz * uz;
+    const float Tuzz = Gxzz * ux + Gyzz * uy + Gz * uz;
+    const float Tuxy = Gxxy * ux + Gxyy * uy + Gxyz * uz;
+    const float Tuxz = Gxxz * ux + Gxyz * uy + Gxzz * uz;
+    const float Tuyz = Gxyz * ux + Gyyz * uy + Gyzz * uz;
+    const float Tuux = Tuxx * ux + Tuxy * uy + Tuxz * uz;
+    const float Tuuy = Tuxy * ux + Tuyy * uy + Tuyz * uz;
+    const float Tuuz = Tuxz * ux + Tuyz * uy + Tuzz * uz;
+    const float Tax = Gx * axx + Gxyy * ayy + Gxzz * azz + 2.0f * (Gxxy * axy + Gxxz * axz + Gxyz * ayz);
+    const float Tay = Gxxy * axx + Gy * ayy + Gyzz * azz + 2.0f * (Gxyy * axy + Gxyz * axz + Gyyz * ayz);
+    const float Taz = Gxxz * axx + Gyyz * ayy + Gz * azz + 2.0f * (Gxyz * axy + Gxzz * axz + Gyzz * ayz);
+    // sum Eh cu^2, sum Eh cac, sum Oh cu, sum Oh cu^3, sum Oh cu cac, -sum Oh cau
+    float R45h = Gux * ux + Guy * uy + Guz * uz;
+    const float K45h = Gxx * axx + Gyy * ayy + Gzz * azz + 2.0f * (Gxy * axy + Gxz * axz + Gyz * ayz);
+    const float D0h = Gx * ux + Gy * uy + Gz * uz;
+    const float R45oh = Tuux * ux + Tuuy * uy + Tuuz * uz;
+    const float K135h = Tuxx * axx + Tuyy * ayy + Tuzz * azz + 2.0f * (Tuxy * axy + Tuxz * axz + Tuyz * ayz);
+    const float K9h = -(Gx * vx + Gy * vy + Gz * vz);
+    // cu^h = 2 R45 Eh cu + Oh (D0 + 3 R45o cu^2 + K135 cac), summed with c
+    uxh += 2.0f * R45 * Gux + D0 * Gx + 3.0f * R45o * Tuux + K135 * Tax;
+    uyh += 2.0f * R45 * Guy + D0 * Gy + 3.0f * R45o * Tuuy + K135 * Tay;
+    uzh += 2.0f * R45 * Guz + D0 * Gz + 3.0f * R45o * Tuuz + K135 * Taz;
+    // cac^h = K45 Eh + K135 Oh cu, summed with c c (off-diagonal entries twice)
+    float axxh = K45 * Gxx + K135 * Tuxx;
+    float ayyh = K45 * Gyy + K135 * Tuyy;
+    float azzh = K45 * Gzz + K135 * Tuzz;
+    float axyh = 2.0f * (K45 * Gxy + K135 * Tuxy);
+    float axzh = 2.0f * (K45 * Gxz + K135 * Tuxz);
+    float ayzh = 2.0f * (K45 * Gyz + K135 * Tuyz);
+    // cau^h = -K9 Oh, summed with c
+    const float vxh = -K9 * Gx, vyh = -K9 * Gy, vzh = -K9 * Gz;
     // v = a u
     axxh += vxh * ux;
     ayyh += vyh * uy;
