@@ -408,14 +408,17 @@ __global__ void __launch_bounds__(128) k_inflow_adj(Acc f, float* uvelh, float r
 }
 
 // reverse of k_periodic (same grid): both ghost planes of the axis pass their
-// adjoints to the planes they were copied from; loads before stores.
+// adjoints to the planes they were copied from; loads before stores.  skipj:
+// leave out the ghost rows j = 0, ny+1 (an accessor that wraps j maps them onto
+// rows ny, 1, which other threads handle).
 template <typename Acc>
-__global__ void k_periodic_adj(Acc a, int axis, int nl) {
+__global__ void k_periodic_adj(Acc a, int axis, int nl, int skipj) {
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int l = blockIdx.z;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int s = blockIdx.y;
     if (l >= nl) return;
+    if (skipj && ((axis == 0 && (t == 0 || t == ny + 1)) || (axis == 2 && (s == 0 || s == ny + 1)))) return;
     int n;
     float *g0, *g1, *sn, *s1;     // ghost 0, ghost n+1, their sources n and 1
     if (axis == 0) {

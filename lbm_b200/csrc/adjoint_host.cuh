@@ -8,9 +8,11 @@
 namespace {
 
 // boundarycond in reverse: the launches of run_bc in the opposite order, each
-// with the adjoint accessor (a copy becomes an accumulation into its source)
+// with the adjoint accessor (a copy becomes an accumulation into its source).
+// wrap: the accessors read periodic j ghost rows as rows ny and 1, so the j copies
+// are identities (left out) and the other copies skip those rows.
 template <int Q, typename AdjA>
-int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
+int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh, bool wrap = false) {
     const int nx = c->p.nx, ny = c->p.ny, nz = c->p.nz, nl = c->p.nl;
     cudaStream_t s = c->stream;
     auto periodic = [&](int axis) {
@@ -18,12 +20,12 @@ int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
         if (axis == 0) grd = dim3((ny + 2 + 127) / 128, nz + 2, nl);
         else if (axis == 1) grd = dim3((nx + 2 + 127) / 128, nz + 2, nl);
         else grd = dim3((nx + 2 + 127) / 128, ny + 2, nl);
-        k_periodic_adj<AdjA><<<grd, 128, 0, s>>>(a1, axis, nl);
+        k_periodic_adj<AdjA><<<grd, 128, 0, s>>>(a1, axis, nl, wrap ? 1 : 0);
         c->launches++;
     };
     const int codes[3] = {c->p.ibnd, c->p.jbnd, c->p.kbnd};
     for (int a = 2; a >= 0; --a)
-        if (codes[a] == 0) periodic(a);
+        if (codes[a] == 0 && !(wrap && a == 1)) periodic(a);
     if (c->p.ibnd == 1) {
         k_inflow_adj<Q, AdjA><<<dim3((ny + 31) / 32, nz), 32, 0, s>>>(a1, uvelh, c->p.rho0, c->cosd, c->sind);
         c->launches++;
@@ -46,7 +48,7 @@ int run_bc_adj(lbm_ctx* c, AdjA a1, AdjA a2, float* uvelh) {
         c->launches++;
     }
     for (int a = 2; a >= 0; --a)
-        if (codes[a] == 0) periodic(a);
+        if (codes[a] == 0 && !(wrap && a == 1)) periodic(a);
     LBM_LAUNCHED(c, "boundarycond adjoint");
     return LBM_OK;
 }
@@ -165,22 +167,49 @@ int lbm_state_adjoint_step(lbm_ctx* c, float* W, float* A, const void* P, int32_
     LBM_TRY(sadj_check(c, "state_adjoint_step"));
     const SoaGrid& g = c->sg;
     const int Q = c->p.nl;
-    const unsigned shell = (unsigned)((sadj_shell_cells(g) + 127) / 128);
+    const int wrap = (c->p.jbnd == 0) ? 1 : 0;   // the stepped state P has no stored j ghost rows
+    // The adjoint arrays may read their j ghost rows as rows ny and 1 too, which
+    // leaves out the j copies, unless the i and k faces are both closed: then the
+    // closed-k kernel reads, through a j ghost row, an x-ghost value of row ny that
+    // the closed-i kernel has overwritten since the first j copy.
+    const int awrap = (wrap && !(c->face_on[0] && c->face_on[2])) ? 1 : 0;
     const dim3 inner((g.nx + 127) / 128, g.ny, g.nz);
-    if (Q == 27) k_sadj_shell<27><<<shell, 128, 0, c->stream>>>(W, A, g);
-    else k_sadj_shell<19><<<shell, 128, 0, c->stream>>>(W, A, g);
-    c->launches++;
-    LBM_LAUNCHED(c, "state adjoint: shell");
-    SoaAdjAcc a1{W, g}, a2{A, g};
-    LBM_TRY(Q == 27 ? run_bc_adj<27>(c, a1, a2, uvelhat) : run_bc_adj<19>(c, a1, a2, uvelhat));
-    const int wrap = (c->p.jbnd == 0) ? 1 : 0;
+    SoaAdjAcc a1{W, g, awrap}, a2{A, g, awrap};
+    if (c->fold && awrap && g.nx >= 2) {
+        // inflow/outflow i, periodic j, closed k: the reverse boundary chain is the
+        // inflow adjoint then the closed-k adjoint, with the x faces in one kernel
+        const unsigned nshell = (unsigned)((sadj_shell_fold_cells(g) + 127) / 128);
+        const dim3 xf((g.ny + 31) / 32, Q, g.nz);
+        if (Q == 27) {
+            k_sadj_shell_fold<27><<<nshell, 128, 0, c->stream>>>(W, A, g);
+            k_sadj_xface<27><<<xf, 32, 0, c->stream>>>(W, A, g, uvelhat, c->p.rho0, c->cosd, c->sind);
+        } else {
+            k_sadj_shell_fold<19><<<nshell, 128, 0, c->stream>>>(W, A, g);
+            k_sadj_xface<19><<<xf, 32, 0, c->stream>>>(W, A, g, uvelhat, c->p.rho0, c->cosd, c->sind);
+        }
+        c->launches += 2;
+        if (c->face_on[2]) {
+            k_closed_adj<SoaAdjAcc><<<dim3((g.nx + 127) / 128, g.ny, 2), 128, 0, c->stream>>>(a1, a2, 2, c->face[2][0],
+                                                                                           c->face[2][1]);
+            c->launches++;
+        }
+        LBM_LAUNCHED(c, "state adjoint: boundaries");
+    } else {
+        const unsigned shell = (unsigned)((sadj_shell_cells(g, awrap != 0) + 127) / 128);
+        if (Q == 27) k_sadj_shell<27><<<shell, 128, 0, c->stream>>>(W, A, g, awrap);
+        else k_sadj_shell<19><<<shell, 128, 0, c->stream>>>(W, A, g, awrap);
+        c->launches++;
+        LBM_LAUNCHED(c, "state adjoint: shell");
+        LBM_TRY(Q == 27 ? run_bc_adj<27>(c, a1, a2, uvelhat, awrap != 0)
+                        : run_bc_adj<19>(c, a1, a2, uvelhat, awrap != 0));
+    }
     const float* Pf = static_cast<const float*>(P);
     if (Q == 27) {
-        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
     } else {
-        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, c->d_solid, c->cp, c->d_abl);
+        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
+        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
     }
     c->launches++;
     LBM_LAUNCHED(c, "state adjoint: collision");

@@ -319,11 +319,15 @@ def test_state_layout_sweep_matches_fp64_finite_differences(nl):
     fb.close()
 
 
-@pytest.mark.parametrize("codes", [(11, 22, 12), (0, 0, 0), (1, 11, 22), (0, 12, 0)])
+@pytest.mark.parametrize("codes", [(11, 22, 12), (0, 0, 0), (1, 11, 22), (0, 12, 0), (11, 0, 22), (1, 0, 0),
+                                   (1, 0, 21), (1, 0, 12)])
 @pytest.mark.parametrize("nl", [19, 27])
 def test_state_layout_sweep_matches_per_call_sweep_for_boundary_codes(codes, nl):
     """Closed faces, edges and corners, periodic axes and inflow: the boundary
-    adjoint reaches the cells next to every face."""
+    adjoint reaches the cells next to every face.  With periodic j the state
+    adjoint reads ghost rows as rows ny and 1 (no j copies); closed i and k with
+    periodic j make edges along j; inflow i, periodic j and closed k take the
+    folded boundary adjoint."""
     ib, jb, kb = codes
     wl = CASE.with_(nl=nl, ibnd=ib, jbnd=jb, kbnd=kb, steps=8)
     pb, f1, f2, uvel = problem(wl, 3)
