@@ -47,6 +47,9 @@ def parse():
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
     ap.add_argument("--adjoint", action="store_true",
                     help="checkpointed adjoint sweep of a probe-misfit loss (D3Q19 256x128x128 sphere, 100 steps)")
+    ap.add_argument("--adjoint-step", action="store_true",
+                    help="time one state-layout reverse step (lbm_state_adjoint_step) of the adjoint workload "
+                         "against one fused forward step, on a resident state (about 2.5 GB)")
     ap.add_argument("--accuracy", action="store_true",
                     help="FP16-offset storage error study (city workload) instead of the timing run")
     return ap.parse_args()
@@ -583,8 +586,76 @@ def adjoint_bench(a):
     return 0
 
 
+def adjoint_step_bench(a):
+    """One reverse step of the state-layout sweep (D3Q19 256x128x128 sphere):
+    lbm_state_adjoint_step pulling from a stepped state, timed over K calls,
+    beside one fused forward step.  Algorithmic traffic of the cell kernel:
+    the adjoint gathered (Q floats), the pulled state (Q) and the adjoint
+    written (Q) per interior cell."""
+    import torch
+    from lbm_b200 import Params, workloads as W
+    from lbm_b200.adjoint import FusedProbeProblem, ProbeProblem, initial_state
+    torch.cuda.set_device(0)
+    wl = W.ADJOINT_Q19
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=10,
+               kinevisc=wl.kinevisc)
+    blank = torch.from_numpy(W.blanking(wl)).cuda()
+    probes = W.probe_cells(wl, 200, 0)
+    fb = FusedProbeProblem(p, probes, 10, blanking=blank)
+    L = fb.lbm
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(wl))
+    fb.uvel = torch.from_numpy(W.inflow_profile(wl)).cuda()
+    pp = ProbeProblem(p, probes, 10, blanking=blank)
+    f1, f2 = initial_state(pp.lbm, rho, u, v, w, fb.uvel)
+    pp.close()
+    fb._import(f1, f2)
+    del f1, f2
+    L.step(3)
+    P = L.state_scratch()
+    L.state_copy(P)
+    Wt, At = L.empty_state(), L.empty_state()
+    At.normal_(0.0, 1e-3, generator=torch.Generator(device="cuda").manual_seed(1))
+    uh = torch.zeros(wl.nz, dtype=torch.float32, device="cuda")
+    steps, warm = max(1, a.steps if a.steps != 1000 else 50), max(3, a.warmup if a.warmup != 20 else 5)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+    for _ in range(warm):
+        L.state_adjoint_step(Wt, At, P, True, uh)
+        Wt, At = At, Wt
+        L.step(1)
+    torch.cuda.synchronize()
+    e0, e1, e2 = ev(), ev(), ev()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record()
+        for _ in range(steps):
+            L.state_adjoint_step(Wt, At, P, True, uh)
+            Wt, At = At, Wt
+        e1.record()
+        L.step(steps)
+        e2.record()
+        torch.cuda.synchronize()
+    t_rev, t_fwd = e0.elapsed_time(e1) / steps, e1.elapsed_time(e2) / steps
+    cells = wl.cells
+    hbm, hbm_kind = peaks()
+    line = {"metric": "state-layout reverse step time over fused forward step time", "value": round(t_rev / t_fwd, 3),
+            "unit": "x", "n_gpus": 1, "steps": steps, "warmup": warm, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded state and adjoint)",
+            "config": {"workload": "adjoint_step_" + wl.name, "grid": [wl.nx, wl.ny, wl.nz], "lattice": "D3Q19",
+                       "l2": "inputs larger than L2 (3 x 331 MB per step)"},
+            "reverse_step_ms": round(t_rev, 4), "fused_step_ms": round(t_fwd, 4),
+            "reverse_step_bytes_per_cell": 3 * wl.nl * 4,
+            "reverse_step_gbs_of_cell_traffic": round(3 * wl.nl * 4 * cells / (t_rev * 1e-3) / 1e9, 1),
+            "hbm_peak_gbs": hbm, "hbm_peak_kind": hbm_kind, "clocks": clk.report()}
+    print(json.dumps(line), flush=True)
+    fb.close()
+    return 0
+
+
 def main():
     a = parse()
+    if a.adjoint_step and a.impl == "ours":
+        return adjoint_step_bench(a)
     if a.adjoint and a.impl == "ours":
         return adjoint_bench(a)
     if a.ensemble and a.impl == "ours":
