@@ -508,11 +508,19 @@ int step_one(lbm_ctx* c) {
 void take_dst(lbm_ctx* c, void* dst) {
     void* prev = c->buf[1 - c->cur];
     if (prev != dst) {
-        const dim3 grd((unsigned)((ghost_cells(c->sg) + 127) / 128), (unsigned)c->p.nl);
-        if (c->elem == 2)
-            k_copy_ghosts<uint16_t><<<grd, 128, 0, c->stream>>>((uint16_t*)dst, (const uint16_t*)prev, c->sg);
-        else
-            k_copy_ghosts<uint32_t><<<grd, 128, 0, c->stream>>>((uint32_t*)dst, (const uint32_t*)prev, c->sg);
+        if (c->fold) {
+            const dim3 grd((unsigned)((fold_ghost_cells(c->sg) + 127) / 128), (unsigned)c->p.nl);
+            if (c->elem == 2)
+                k_copy_ghosts_fold<uint16_t><<<grd, 128, 0, c->stream>>>((uint16_t*)dst, (const uint16_t*)prev, c->sg);
+            else
+                k_copy_ghosts_fold<uint32_t><<<grd, 128, 0, c->stream>>>((uint32_t*)dst, (const uint32_t*)prev, c->sg);
+        } else {
+            const dim3 grd((unsigned)((ghost_cells(c->sg) + 127) / 128), (unsigned)c->p.nl);
+            if (c->elem == 2)
+                k_copy_ghosts<uint16_t><<<grd, 128, 0, c->stream>>>((uint16_t*)dst, (const uint16_t*)prev, c->sg);
+            else
+                k_copy_ghosts<uint32_t><<<grd, 128, 0, c->stream>>>((uint32_t*)dst, (const uint32_t*)prev, c->sg);
+        }
         c->launches++;
     }
     c->buf[1 - c->cur] = dst;

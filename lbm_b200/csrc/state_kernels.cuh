@@ -276,6 +276,39 @@ __global__ void __launch_bounds__(128) k_copy_ghosts(T* __restrict__ dst, const 
     dst[o] = src[o];
 }
 
+// k_copy_ghosts for the folded configuration, which reads fewer ghost entries of
+// a buffer: the k ghost rows (j = 1..ny, every i; exports read them whole) and the
+// x ghosts of the rows k = 1 and nz (the boundary kernel reads them two steps
+// after they were written).  The other x ghosts are rewritten by every step where
+// a step reads them and exported from the compact x-ghost arrays, and periodic j
+// rows are read as rows ny and 1.  A thread per cell, blockIdx.y = direction.
+template <typename T>
+__global__ void __launch_bounds__(128) k_copy_ghosts_fold(T* __restrict__ dst, const T* __restrict__ src, SoaGrid g) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const long long nrow = 2LL * ny * (nx + 2);
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int i, j, k;
+    if (t < nrow) {
+        const long long r = t / (nx + 2);
+        i = (int)(t - r * (nx + 2));
+        j = 1 + (int)(r % ny);
+        k = (r < ny) ? 0 : nz + 1;
+    } else {
+        const long long u = t - nrow;
+        const int nk = (nz > 1) ? 2 : 1;
+        if (u >= 2LL * nk * ny) return;
+        i = (u & 1) ? nx + 1 : 0;
+        const long long r = u >> 1;
+        j = 1 + (int)(r % ny);
+        k = (r < ny) ? 1 : nz;
+    }
+    const long long o = (long long)blockIdx.y * g.dstride + g.off(i, j, k);
+    dst[o] = src[o];
+}
+inline long long fold_ghost_cells(const SoaGrid& g) {
+    return 2LL * g.ny * (g.nx + 2) + 2LL * ((g.nz > 1) ? 2 : 1) * g.ny;
+}
+
 // The ghost shell of a state buffer to or from a compact array
 // packed[l][t] (t: ghost_cell numbering).  UNPACK: packed -> buffer.
 template <typename T, bool UNPACK>
