@@ -183,8 +183,11 @@ inline long long sadj_shell_fold_cells(const SoaGrid& g) {
 // cells i = 1 and nx are written, not accumulated: nothing earlier in the
 // reverse step reaches them.  The inflow ghost of a direction l with cx > 0 is
 // its opposite's corrected value, so the thread of a direction s with cx < 0
-// also consumes the ghost adjoint of opp(s).  Grid: x over j (32 per block),
-// y = direction, z = k; uvelh(k) gets one atomic per warp.
+// also consumes the ghost adjoint of opp(s).  Between the rows k = 2 and nz-1
+// the x-ghost adjoints are zero when this kernel runs (only the closed-k adjoint
+// adds to x ghosts, and only in the rows 1 and nz), so there they are neither
+// read nor cleared.  Grid: x over j (32 per block), y = direction, z = k;
+// uvelh(k) gets one atomic per warp.
 template <int Q>
 __global__ void __launch_bounds__(32) k_sadj_xface(float* __restrict__ W, const float* __restrict__ A, SoaGrid g,
                                                    float* __restrict__ uvelh, float rho0, float cosd, float sind) {
@@ -196,28 +199,31 @@ __global__ void __launch_bounds__(32) k_sadj_xface(float* __restrict__ W, const 
         const int cx = c_cx[l], cy = c_cy[l], cz = c_cz[l];
         const long long dl = (long long)l * g.dstride;
         const long long o0 = g.off(0, j, k), on = g.off(nx, j, k);
+        const bool kface = (k == 1 || k == nz);      // x-ghost adjoints may be nonzero
         // outflow: f(l, nx+1) = f(l, nx); the ghost's adjoint includes its pull (cx < 0)
-        float vo = W[dl + on + 1];
+        float vo = kface ? W[dl + on + 1] : 0.0f;
         if (cx < 0 && k + cz >= 1 && k + cz <= nz)
             vo += A[dl + g.off(nx, wrapj(j + cy, ny), k + cz)];
         // inflow ghosts at i = 0 whose source is direction l (cx <= 0): l itself and, for cx < 0, opp(l)
         float acc = 0.0f, vi = 0.0f, vp = 0.0f;
         int lo = l;
         if (cx <= 0) {
-            vi = W[dl + o0];
+            if (kface) vi = W[dl + o0];
             if (cx < 0) {
                 lo = c_opp[l];
                 const long long dlo = (long long)lo * g.dstride;
-                vp = W[dlo + o0];
+                if (kface) vp = W[dlo + o0];
                 if (k - cz >= 1 && k - cz <= nz) vp += A[dlo + g.off(1, wrapj(j - cy, ny), k - cz)];
             }
             acc = vi + vp;
         }
-        W[dl + on + 1] = 0.0f;
+        if (kface) {
+            W[dl + on + 1] = 0.0f;
+            if (cx <= 0) W[dl + o0] = 0.0f;
+            if (cx < 0) W[(long long)lo * g.dstride + o0] = 0.0f;
+        }
         W[dl + on] = vo;
         if (cx <= 0) {
-            W[dl + o0] = 0.0f;
-            if (cx < 0) W[(long long)lo * g.dstride + o0] = 0.0f;
             const float wl = c_w[Q == 27 ? 1 : 0][l];
             uh = -acc * 2.0f * wl * rho0 * ((float)cx * cosd + (float)cy * sind) * 3.0f;
         }
