@@ -546,6 +546,15 @@ def adjoint_bench(a):
     torch.cuda.synchronize()
     ts_fwd, ts_bwd = s0.elapsed_time(s1), s1.elapsed_time(s2)
     agree = float((sf - gf).abs().max() / gf.abs().max())
+    # the same reverse sweep with replay and reverse one after the other
+    s3, s4 = ev(), ev()
+    s3.record()
+    tf, tu = fb.backward(2.0 * (us - truth), overlap=False)
+    s4.record()
+    torch.cuda.synchronize()
+    ts_serial = s3.elapsed_time(s4)
+    agree_serial = float((tf - gf).abs().max() / gf.abs().max())
+    del tf, tu
     fb.close()
     del sf, su
     torch.cuda.empty_cache()
@@ -574,10 +583,14 @@ def adjoint_bench(a):
             "state_layout_sweep": {"forward_ms": round(ts_fwd, 2), "reverse_ms": round(ts_bwd, 2),
                                    "reverse_over_forward": round(ts_bwd / ts_fwd, 3),
                                    "reverse_over_fused_forward": round(ts_bwd / t_fused, 3),
+                                   "reverse_ms_without_overlap": round(ts_serial, 2),
+                                   "gradient_without_overlap_vs_per_call_sweep": agree_serial,
                                    "gradient_vs_per_call_sweep": agree,
                                    "how": "forward by the fused step with a device snapshot every 10 steps "
                                           "(lbm_state_snapshot); reverse restores each segment, replays it "
-                                          "into per-step buffers (lbm_step_to) and runs lbm_state_adjoint_step"},
+                                          "into per-step buffers (lbm_step_to) on a second context and stream "
+                                          "while the adjoint steps of the segment after it run "
+                                          "(lbm_state_adjoint_step)"},
             "forward_mlups": round(cells * wl.steps / (t_fwd * 1e-3) / 1e6, 1),
             "loss": loss, "grad_norm": {"f1": gnorm_f, "uvel": gnorm_u},
             "gradient_check": "tests/test_gpu_adjoint.py: central FP64 differences, 8 seeded directions, rel <= 1e-4",

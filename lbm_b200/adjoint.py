@@ -117,6 +117,9 @@ class ProbeProblem:
 
     def close(self):
         self.ckpt = {}
+        if getattr(self, "_rep", None) is not None:
+            self._rep.close()
+            self._rep = None
         self.lbm.close()
 
 
@@ -177,35 +180,90 @@ class FusedProbeProblem:
         L.get_macro(*R)
         return torch.stack([R[q].reshape(-1)[self.pidx] for q in (1, 2, 3)], dim=1)
 
-    def backward(self, uhat_probes):
+    def _replayer(self):
+        """The context that replays segments, on a stream of its own with a higher
+        priority than the adjoint's, so a replay runs beside the adjoint steps of
+        the segment after it (the replay is DRAM-bound, the adjoint cell kernel
+        issue-bound)."""
+        if getattr(self, "_rep", None) is None:
+            stream = torch.cuda.Stream(priority=-1)
+            self._rep = Lbm(self.p, stream=stream)
+            if self.blanking is not None:
+                self._rep.set_solids(self.blanking)
+        return self._rep
+
+    def backward(self, uhat_probes, overlap: bool = True):
+        """Gradient of the probe loss with respect to the initial f1 and the inflow
+        profile.  overlap: replay segment q+1 (on the replay context's stream, into
+        the other of two sets of state arrays) while the adjoint steps of segment q
+        run; otherwise replay and reverse one segment after the other."""
         L = self.lbm
         W, A = L.empty_state(), L.empty_state()
         uvel_h = torch.zeros(self.p.nz, dtype=torch.float32, device="cuda")
-        for s in sorted(self.ckpt, reverse=True):
+        segs = sorted(self.ckpt, reverse=True)
+        R = self._replayer() if overlap else L
+        main = L.stream
+        rep = R.stream
+        rep.wait_stream(main)                # the forward's snapshots and the seed are written on main
+        R.set_inflow(self.uvel)
+        nsets = 2 if overlap else 1
+        sets = [[L.state_scratch() for _ in range(self.K)] for _ in range(nsets)]
+        firsts = [L.state_scratch() for _ in range(nsets)]
+        released = [None] * nsets            # event: the adjoint is done with a set
+
+        def replay(q):
+            s, b = segs[q], q % nsets
             e = min(s + self.K, self.nsteps)
-            if s == 0:
-                self._import(*self.ckpt[s])
-                first = L.state_scratch()
-                L.state_copy(first)           # the imported f1: input of step 0
-            else:
-                first = self.ckpt[s]          # the state after step s - 1, which step s pulls from
-                L.restore(first)
-                L.set_inflow(self.uvel)
-            P = []
-            for _ in range(s, e):
-                P.append(L.state_scratch())
-                L.step_to(P[-1])              # the step writes its state into P[-1]
-            if e == self.nsteps:
-                L.state_adjoint_seed(A, P[-1], self.probes_dev, uhat_probes.float())
-            for n in range(e - 1, s - 1, -1):
-                src = P[n - s - 1] if n > s else first
-                L.state_adjoint_step(W, A, src, n > s or s > 0, uvel_h)
-                W, A = A, W                   # A: adjoint of f1 before step n, W: of f2
-            del P, first
+            with torch.cuda.stream(rep):
+                if released[b] is not None:
+                    rep.wait_event(released[b])
+                if s == 0:
+                    Rm = [R.empty_s() for _ in range(4)]
+                    f1, f2 = self.ckpt[0]
+                    R.macrovars(*Rm, f1)
+                    R.state_import(f1, f2, *Rm)
+                    R.state_copy(firsts[b])  # the imported f1: input of step 0
+                    first = firsts[b]
+                else:
+                    first = self.ckpt[s]     # the state after step s - 1, which step s pulls from
+                    R.restore(first)
+                for n in range(s, e):
+                    R.step_to(sets[b][n - s])  # the step writes its state into the array
+                ready = torch.cuda.Event()
+                ready.record(rep)
+            return first, ready
+
+        # The adjoint steps of segment q are enqueued before the replay of q + 1:
+        # restoring a snapshot reads its header on the host, which waits for the
+        # replay stream, so the main stream must already hold work by then.
+        pending = replay(0)
+        for q, s in enumerate(segs):
+            b = q % nsets
+            e = min(s + self.K, self.nsteps)
+            first, ready = pending
+            main.wait_event(ready)
+            P = sets[b]
+            with torch.cuda.stream(main):
+                if e == self.nsteps:
+                    L.state_adjoint_seed(A, P[e - s - 1], self.probes_dev, uhat_probes.float())
+                for n in range(e - 1, s - 1, -1):
+                    src = P[n - s - 1] if n > s else first
+                    L.state_adjoint_step(W, A, src, n > s or s > 0, uvel_h)
+                    W, A = A, W               # A: adjoint of f1 before step n, W: of f2
+                done = torch.cuda.Event()
+                done.record(main)
+            released[b] = done
+            if q + 1 < len(segs):
+                pending = replay(q + 1)
         g = L.empty_f()
         L.state_adjoint_export(g, A)
+        main.synchronize()
+        del sets, firsts
         return g, uvel_h
 
     def close(self):
         self.ckpt = {}
+        if getattr(self, "_rep", None) is not None:
+            self._rep.close()
+            self._rep = None
         self.lbm.close()
