@@ -23,12 +23,18 @@ namespace lbm {
 // gh: adjoint of the post-collision populations.  fh receives the adjoint of
 // the pre-collision populations; rh, uxh, uyh, uzh are incremented by the
 // adjoint of postcoll's rho, u, v, w inputs.
+// The reverse of the collision up to the adjoint of its second moments (a_ij,
+// with the trace and the macroscopic inputs): everything collide_adj does except
+// emitting the per-direction adjoint.  m: moments of the pre-collision offsets.
+struct CollideAdjOut {
+    float s0h, axxh, ayyh, azzh, axyh, axzh, ayzh;
+};
 template <int Q>
-__device__ __forceinline__ void collide_adj(const float (&fp)[Q], const float (&gh)[Q], float rho, float ux, float uy,
-                                            float uz, const CollideParams& cp, float abl, float tau_in, float (&fh)[Q],
-                                            float& rh, float& uxh, float& uyh, float& uzh) {
+__device__ __forceinline__ CollideAdjOut collide_adj_moments(const Moments& m, const float (&gh)[Q], float rho, float ux,
+                                                             float uy, float uz, const CollideParams& cp, float abl,
+                                                             float tau_in, float& rh, float& uxh, float& uyh,
+                                                             float& uzh) {
     // ---- forward values (as collide()) ----
-    const Moments m = moments<Q>(fp);
     const float third = 1.0f / 3.0f;
     const float rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
     const float axx = m.pxx - m.s0 * third - rux * ux;
@@ -189,17 +195,25 @@ __device__ __forceinline__ void collide_adj(const float (&fp)[Q], const float (&
     uxh -= rho * (2.0f * ux * axxh + uy * axyh + uz * axzh);
     uyh -= rho * (2.0f * uy * ayyh + ux * axyh + uz * ayzh);
     uzh -= rho * (2.0f * uz * azzh + ux * axzh + uy * ayzh);
+    return CollideAdjOut{s0h, axxh, ayyh, azzh, axyh, axzh, ayzh};
+}
+
+template <int Q>
+__device__ __forceinline__ void collide_adj(const float (&fp)[Q], const float (&gh)[Q], float rho, float ux, float uy,
+                                            float uz, const CollideParams& cp, float abl, float tau_in, float (&fh)[Q],
+                                            float& rh, float& uxh, float& uyh, float& uzh) {
+    const CollideAdjOut o = collide_adj_moments<Q>(moments<Q>(fp), gh, rho, ux, uy, uz, cp, abl, tau_in, rh, uxh, uyh, uzh);
     // moments are linear in f
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-        float v = s0h;
-        macc(v, cx * cx, axxh);
-        macc(v, cy * cy, ayyh);
-        macc(v, cz * cz, azzh);
-        macc(v, cx * cy, axyh);
-        macc(v, cx * cz, axzh);
-        macc(v, cy * cz, ayzh);
+        float v = o.s0h;
+        macc(v, cx * cx, o.axxh);
+        macc(v, cy * cy, o.ayyh);
+        macc(v, cz * cz, o.azzh);
+        macc(v, cx * cy, o.axyh);
+        macc(v, cx * cz, o.axzh);
+        macc(v, cy * cz, o.ayzh);
         fh[l] = v;
     }
 }

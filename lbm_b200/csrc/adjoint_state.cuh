@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
     if (i > g.nx) return;
     const long long o = g.off(i, j, k);
-    float fp[Q], gh[Q], fh[Q];
+    float fp[Q], gh[Q];
     if (PULL) {
         PullMacro<Q, float, 0>::run(fp, P, g, o, j, wrap != 0);
     } else {
@@ -276,21 +276,32 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
             gh[l + 1] = x;
         }
     }
-    const Moments m = moments<Q>(fp);
+    const Moments m = moments_rows<Q>(fp);
     const float rho = 1.0f + m.s0;
     const float ux = m.jx / rho, uy = m.jy / rho, uz = m.jz / rho;
     float rh = 0.f, uxh = 0.f, uyh = 0.f, uzh = 0.f;
-    collide_adj<Q>(fp, gh, rho, ux, uy, uz, cp, abl ? abl[k - 1] : 0.0f, cp.tau0, fh, rh, uxh, uyh, uzh);
-    // rho = sum f, u = (sum c f) / rho
+    const CollideAdjOut c = collide_adj_moments<Q>(m, gh, rho, ux, uy, uz, cp, abl ? abl[k - 1] : 0.0f, cp.tau0, rh,
+                                                   uxh, uyh, uzh);
+    // rho = sum f, u = (sum c f) / rho; the adjoint of f_l is E +- O over the
+    // opposite pair (l, l+1): E = s0h + rh - a.u + c c : a_h, O = c . a
     const float ax = uxh / rho, ay = uyh / rho, az = uzh / rho;
-    const float base = rh - (ax * ux + ay * uy + az * uz);
+    const float E0 = c.s0h + rh - (ax * ux + ay * uy + az * uz);
+    W[o] = E0;
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        float d = base;
-        macc(d, lat_cx(l), ax);
-        macc(d, lat_cy(l), ay);
-        macc(d, lat_cz(l), az);
-        W[(long long)l * g.dstride + o] = fh[l] + d;
+    for (int l = 1; l < Q; l += 2) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        float E = E0, O = 0.0f;
+        macc(E, cx * cx, c.axxh);
+        macc(E, cy * cy, c.ayyh);
+        macc(E, cz * cz, c.azzh);
+        macc(E, cx * cy, c.axyh);
+        macc(E, cx * cz, c.axzh);
+        macc(E, cy * cz, c.ayzh);
+        macc(O, cx, ax);
+        macc(O, cy, ay);
+        macc(O, cz, az);
+        W[(long long)l * g.dstride + o] = E + O;
+        W[(long long)(l + 1) * g.dstride + o] = E - O;
     }
 }
 
