@@ -46,6 +46,7 @@ __device__ __forceinline__ CollideAdjOut collide_adj_moments(const Moments& m, c
     const float tr = axx + ayy + azz;
     float tau = tau_in;
     float amag0 = 0.f, amag = 0.f, b11 = 0.f, b22 = 0.f, b33 = 0.f, b12 = 0.f, b13 = 0.f, b23 = 0.f, bb = 0.f, t = 0.f;
+    float iamag = 0.f, st = 0.f;   // 1 / amag, sqrt(t)
     if (cp.ivreman) {
         amag0 = axx * axx + ayy * ayy + azz * azz + 2.0f * (axy * axy + axz * axz + ayz * ayz);
         amag = fmaxf(amag0, 1.17549435e-38f);
@@ -56,11 +57,14 @@ __device__ __forceinline__ CollideAdjOut collide_adj_moments(const Moments& m, c
         b13 = cp.eps + axx * axz + axy * ayz + axz * azz;
         b23 = cp.eps + axy * axz + ayy * ayz + ayz * azz;
         bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
-        t = bb / amag;
-        const float nut = (t > cp.eps) ? cp.cvre * sqrtf(t) : 0.0f;
+        iamag = 1.0f / amag;
+        t = bb * iamag;
+        st = sqrtf(t);
+        const float nut = (t > cp.eps) ? cp.cvre * st : 0.0f;
         tau = 3.0f * (cp.kinevisc + nut + abl) + 0.5f;
     }
-    const float K = 1.0f - 1.0f / tau;
+    const float itau = 1.0f / tau;
+    const float K = 1.0f - itau;
     const bool cubic = (cp.ibgk == 3);
     const float usq = ux * ux + uy * uy + uz * uz;
     const float R45 = 4.5f * rho;
@@ -176,10 +180,10 @@ __device__ __forceinline__ CollideAdjOut collide_adj_moments(const Moments& m, c
     azzh += trh;
     // K = 1 - 1/tau, tau = 3 (nu + nut + abl) + 1/2, nut = cvre sqrt(bb / amag) where bb / amag > eps
     if (cp.ivreman && t > cp.eps) {
-        const float nuth = 3.0f * Kh / (tau * tau);
-        const float th = nuth * cp.cvre * 0.5f / sqrtf(t);
-        const float bbh = th / amag;
-        const float amagh = (amag0 >= 1.17549435e-38f) ? -th * bb / (amag * amag) : 0.0f;
+        // dK/dtau = 1/tau^2, dtau/dnut = 3, dnut/dt = cvre / (2 sqrt t), t = bb / amag
+        const float th = 1.5f * Kh * itau * itau * cp.cvre / st;
+        const float bbh = th * iamag;
+        const float amagh = (amag0 >= 1.17549435e-38f) ? -bbh * t : 0.0f;
         const float b11h = bbh * (b22 + b33), b22h = bbh * (b11 + b33), b33h = bbh * (b11 + b22);
         const float b12h = -2.0f * b12 * bbh, b13h = -2.0f * b13 * bbh, b23h = -2.0f * b23 * bbh;
         axxh += 2.0f * axx * b11h + axy * b12h + axz * b13h + 2.0f * axx * amagh;

@@ -278,13 +278,14 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
     }
     const Moments m = moments_rows<Q>(fp);
     const float rho = 1.0f + m.s0;
-    const float ux = m.jx / rho, uy = m.jy / rho, uz = m.jz / rho;
+    const float irho = 1.0f / rho;
+    const float ux = m.jx * irho, uy = m.jy * irho, uz = m.jz * irho;
     float rh = 0.f, uxh = 0.f, uyh = 0.f, uzh = 0.f;
     const CollideAdjOut c = collide_adj_moments<Q>(m, gh, rho, ux, uy, uz, cp, abl ? abl[k - 1] : 0.0f, cp.tau0, rh,
                                                    uxh, uyh, uzh);
     // rho = sum f, u = (sum c f) / rho; the adjoint of f_l is E +- O over the
     // opposite pair (l, l+1): E = s0h + rh - a.u + c c : a_h, O = c . a
-    const float ax = uxh / rho, ay = uyh / rho, az = uzh / rho;
+    const float ax = uxh * irho, ay = uyh * irho, az = uzh * irho;
     const float E0 = c.s0h + rh - (ax * ux + ay * uy + az * uz);
     W[o] = E0;
 #pragma unroll
