@@ -172,6 +172,24 @@ int lbm_set_inflow(lbm_ctx* ctx, const float* uvel);
 int lbm_set_forcing(lbm_ctx* ctx, const float* external_forcing);
 /* advance nsteps time steps */
 int lbm_step(lbm_ctx* ctx, int32_t nsteps);
+/* j-slab decomposition of one domain over several contexts (GPUs), as the
+ * reference's MPI tiling (m_mpi_decomp_init.F90:123-134, m_mpi_halo_exchange_j.F90:3-121).
+ * A tile is a context whose ny is the tile's rows; lbm_set_halo_j(ctx, 1), before
+ * the first import, makes it keep stored j ghost planes that the caller fills
+ * (the step reads them instead of wrapping j, the folded boundary path is off).
+ * The boundary conditions of a tile run as in the reference, tile by tile; after
+ * each lbm_step the caller packs planes j = 1 and j = ny of the current state
+ * (all i = 0..nx+1, k = 0..nz+1 and directions; lbm_halo_plane_bytes each),
+ * sends them to the south and north neighbours, and unpacks what it receives
+ * from the south into j = 0 and from the north into j = ny+1 -- the reference's
+ * exchange after boundarycond and before drift (main.F90:310-318).  NULL skips a
+ * plane (no neighbour).  Device buffers; plane layout [l][k][i] of the storage
+ * type. */
+int lbm_set_halo_j(lbm_ctx* ctx, int32_t on);
+int lbm_halo_plane_bytes(lbm_ctx* ctx, int64_t* bytes);
+int lbm_halo_pack_j(lbm_ctx* ctx, void* to_south, void* to_north);
+int lbm_halo_unpack_j(lbm_ctx* ctx, const void* from_south, const void* from_north);
+
 /* Snapshots of a stepped state in device memory: everything a context needs to
  * resume from that step (its state buffer, the ghost shell the next boundaries
  * read, the compact x-ghost columns and the step number).  A snapshot restores

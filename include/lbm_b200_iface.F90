@@ -154,6 +154,24 @@ module lbm_b200_iface
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, dst
       end function
+      integer(c_int) function lbm_set_halo_j(ctx, on) bind(C, name="lbm_set_halo_j")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx
+         integer(c_int32_t), value :: on
+      end function
+      integer(c_int) function lbm_halo_plane_bytes(ctx, bytes) bind(C, name="lbm_halo_plane_bytes")
+         import :: c_ptr, c_int, c_int64_t
+         type(c_ptr), value     :: ctx
+         integer(c_int64_t)     :: bytes
+      end function
+      integer(c_int) function lbm_halo_pack_j(ctx, to_south, to_north) bind(C, name="lbm_halo_pack_j")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, to_south, to_north
+      end function
+      integer(c_int) function lbm_halo_unpack_j(ctx, from_south, from_north) bind(C, name="lbm_halo_unpack_j")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, from_south, from_north
+      end function
       integer(c_int) function lbm_state_snapshot_bytes(ctx, bytes) bind(C, name="lbm_state_snapshot_bytes")
          import :: c_ptr, c_int, c_int64_t
          type(c_ptr), value     :: ctx

@@ -78,6 +78,10 @@ SIGNATURES = {
     "lbm_forcings_apply": [P, P, P, P, P, P, P],
     "lbm_step": [P, I],
     "lbm_step_to": [P, P],
+    "lbm_set_halo_j": [P, I],
+    "lbm_halo_plane_bytes": [P, P],
+    "lbm_halo_pack_j": [P, P, P],
+    "lbm_halo_unpack_j": [P, P, P],
     "lbm_state_snapshot_bytes": [P, P],
     "lbm_state_snapshot": [P, P],
     "lbm_state_restore": [P, P],

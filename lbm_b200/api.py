@@ -315,6 +315,21 @@ class Lbm:
     def step(self, nsteps=1):
         self._call("lbm_step", ctypes.c_int32(nsteps))
 
+    # ---- j slabs (one tile of a domain split in j; lbm_b200.slabs drives them) ----
+    def set_halo_j(self, on: bool = True):
+        self._call("lbm_set_halo_j", ctypes.c_int32(1 if on else 0))
+
+    def halo_plane_bytes(self) -> int:
+        n = ctypes.c_int64(0)
+        self._call("lbm_halo_plane_bytes", ctypes.byref(n))
+        return int(n.value)
+
+    def halo_pack_j(self, to_south, to_north):
+        self._call("lbm_halo_pack_j", _ptr(to_south), _ptr(to_north))
+
+    def halo_unpack_j(self, from_south, from_north):
+        self._call("lbm_halo_unpack_j", _ptr(from_south), _ptr(from_north))
+
     def snapshot_bytes(self) -> int:
         n = ctypes.c_int64(0)
         self._call("lbm_state_snapshot_bytes", ctypes.byref(n))

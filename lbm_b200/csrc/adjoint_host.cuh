@@ -156,6 +156,7 @@ static int sadj_check(lbm_ctx* c, const char* what) {
     if (c->p.ihrr != 1) return fail(c, LBM_ERR_UNSUPPORTED, "%s: the regularized collision (ihrr = 1) only", what);
     if (c->nrturb > 0) return fail(c, LBM_ERR_UNSUPPORTED, "%s: no inflow-turbulence slice", what);
     if (c->force) return fail(c, LBM_ERR_UNSUPPORTED, "%s: no external forcing", what);
+    if (c->halo_j) return fail(c, LBM_ERR_UNSUPPORTED, "%s: a whole domain (no j slab)", what);
     return LBM_OK;
 }
 

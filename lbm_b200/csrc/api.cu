@@ -60,6 +60,8 @@ struct lbm_ctx {
     int nrturb = 0;
     float ampl = 0.f;
     bool fold = false;            // boundaries folded into the step kernel (see state_kernels.cuh)
+    bool fold_cfg = false;        // the boundary codes allow folding (fold unless halo_j)
+    bool halo_j = false;          // j ghost planes filled by the caller's halo exchange (lbm_set_halo_j)
     void* d_edge = nullptr;       // populations at i=1 and i=nx of the latest step
     void* d_xg[2] = {nullptr, nullptr};  // compact x-ghost columns of each buffer (folded boundaries)
     bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
@@ -275,7 +277,8 @@ void setup_boundaries(lbm_ctx* c) {
     // the reference's configuration (inflow/outflow i, periodic j, closed k) runs with folded boundaries
     int ko1, koN;
     closed_opts(kb, ko1, koN);
-    c->fold = (ib == 1 && jb == 0 && ko1 != 0);
+    c->fold_cfg = (ib == 1 && jb == 0 && ko1 != 0);
+    c->fold = c->fold_cfg && !c->halo_j;
     c->kopt_lo = ko1;
     c->kopt_hi = koN;
     // m_boundary_i_inflow_kernel.F90:191-193: cos(udir*pi/180), sin(udir*pi/180) in single precision
@@ -550,7 +553,7 @@ void launch_import(lbm_ctx* c, const float* ref, int b) {
 template <typename S>
 const S* xg_of(const lbm_ctx* c, int b) { return c->fold ? (const S*)c->d_xg[b] : nullptr; }
 // after a step, periodic-j ghost rows are read as rows ny and 1 (state_kernels.cuh)
-int wrap_rows(const lbm_ctx* c) { return (c->state == ST_POST && c->p.jbnd == 0) ? 1 : 0; }
+int wrap_rows(const lbm_ctx* c) { return (c->state == ST_POST && c->p.jbnd == 0 && !c->halo_j) ? 1 : 0; }
 
 template <int Q, typename S>
 void launch_export(lbm_ctx* c, float* ref, int b, bool pull) {
@@ -1112,6 +1115,56 @@ int lbm_state_restore(lbm_ctx* c, const void* src) {
     c->cur = 0;
     c->it = h.it;
     c->state = ST_POST;
+    return LBM_OK;
+}
+
+// ---- j-slab decomposition (m_mpi_halo_exchange_j.F90:3-121, m_mpi_pack_jplane.F90,
+// m_mpi_unpack_jplane.F90) ---------------------------------------------------------
+int lbm_set_halo_j(lbm_ctx* c, int32_t on) {
+    if (!c) return LBM_ERR_ARG;
+    if (c->state != ST_NONE) return fail(c, LBM_ERR_STATE, "set_halo_j: call it before the first import");
+    c->halo_j = (on != 0);
+    c->fold = c->fold_cfg && !c->halo_j;
+    return LBM_OK;
+}
+
+int lbm_halo_plane_bytes(lbm_ctx* c, int64_t* bytes) {
+    if (!c || !bytes) return LBM_ERR_ARG;
+    *bytes = (int64_t)c->p.nl * (c->p.nx + 2) * (c->p.nz + 2) * (int64_t)c->elem;
+    return LBM_OK;
+}
+
+static int halo_plane(lbm_ctx* c, void* buf, int j, bool unpack) {
+    const dim3 grd((unsigned)((c->p.nx + 2 + 127) / 128), (unsigned)(c->p.nz + 2), (unsigned)c->p.nl);
+    void* f = c->buf[c->cur];
+    if (c->elem == 2) {
+        if (unpack) k_halo_plane<uint16_t, true><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j);
+        else k_halo_plane<uint16_t, false><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j);
+    } else {
+        if (unpack) k_halo_plane<uint32_t, true><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j);
+        else k_halo_plane<uint32_t, false><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j);
+    }
+    c->launches++;
+    return LBM_OK;
+}
+
+int lbm_halo_pack_j(lbm_ctx* c, void* to_south, void* to_north) {
+    if (!c) return LBM_ERR_ARG;
+    if (!c->halo_j) return fail(c, LBM_ERR_STATE, "halo_pack_j: lbm_set_halo_j(ctx, 1) was not called");
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "halo_pack_j: no state imported");
+    if (to_south) halo_plane(c, to_south, 1, false);
+    if (to_north) halo_plane(c, to_north, c->p.ny, false);
+    LBM_LAUNCHED(c, "halo pack");
+    return LBM_OK;
+}
+
+int lbm_halo_unpack_j(lbm_ctx* c, const void* from_south, const void* from_north) {
+    if (!c) return LBM_ERR_ARG;
+    if (!c->halo_j) return fail(c, LBM_ERR_STATE, "halo_unpack_j: lbm_set_halo_j(ctx, 1) was not called");
+    if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "halo_unpack_j: no state imported");
+    if (from_south) halo_plane(c, const_cast<void*>(from_south), 0, true);
+    if (from_north) halo_plane(c, const_cast<void*>(from_north), c->p.ny + 1, true);
+    LBM_LAUNCHED(c, "halo unpack");
     return LBM_OK;
 }
 

@@ -309,6 +309,20 @@ inline long long fold_ghost_cells(const SoaGrid& g) {
     return 2LL * g.ny * (g.nx + 2) + 2LL * ((g.nz > 1) ? 2 : 1) * g.ny;
 }
 
+// Plane j of a state buffer (every i = 0..nx+1, k = 0..nz+1 and direction) to or
+// from a contiguous array buf[l][k][i]: the halo planes of a j slab.  UNPACK:
+// buf -> buffer.  Grid: x over i, y = k, z = l.
+template <typename T, bool UNPACK>
+__global__ void __launch_bounds__(128) k_halo_plane(T* buf, T* f, SoaGrid g, int j) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > g.nx + 1) return;
+    const int k = blockIdx.y, l = blockIdx.z;
+    const long long q = ((long long)l * (g.nz + 2) + k) * (g.nx + 2) + i;
+    const long long o = (long long)l * g.dstride + g.off(i, j, k);
+    if (UNPACK) f[o] = buf[q];
+    else buf[q] = f[o];
+}
+
 // The ghost shell of a state buffer to or from a compact array
 // packed[l][t] (t: ghost_cell numbering).  UNPACK: packed -> buffer.
 template <typename T, bool UNPACK>
