@@ -47,6 +47,10 @@ def parse():
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
     ap.add_argument("--adjoint", action="store_true",
                     help="checkpointed adjoint sweep of a probe-misfit loss (D3Q19 256x128x128 sphere, 100 steps)")
+    ap.add_argument("--slabs", action="store_true",
+                    help="the default workload as one j slab per rank (tile ny = workload ny) with the halo "
+                         "exchange after every step: NCCL between ranks under torchrun, a ring of one tile "
+                         "with itself on one GPU")
     ap.add_argument("--adjoint-step", action="store_true",
                     help="time one state-layout reverse step (lbm_state_adjoint_step) of the adjoint workload "
                          "against one fused forward step, on a resident state (about 2.5 GB)")
@@ -665,8 +669,75 @@ def adjoint_step_bench(a):
     return 0
 
 
+def slab_bench(a):
+    """MLUPS of j slabs: each rank steps one tile of the default workload's size
+    (weak scaling: the domain grows in j with the ranks) and exchanges its halo
+    planes after every step (lbm_b200.slabs).  Device time with CUDA events,
+    max over ranks."""
+    import torch
+    from lbm_b200 import Params, replicas, slabs, workloads as W
+    from lbm_b200.adjoint import initial_state
+    rank, local, world = replicas.env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        replicas.init("nccl", timeout_s=120, device=torch.device("cuda", local))
+    wl = W.WORKLOADS[a.workload]
+    gp = Params(nx=wl.nx, ny=wl.ny * world, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd,
+                iturb_pos=min(10, wl.nx), kinevisc=wl.kinevisc, smagorinsky=wl.smagorinsky,
+                storage=a.storage)
+    tile = slabs.SlabTile(gp, rank, world)
+    tw = wl.with_(seed=replicas.replica_seed(wl.seed, rank))
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(tw))
+    uvel = torch.from_numpy(W.inflow_profile(tw)).cuda()
+    tile.set_inflow(uvel)
+    f1, f2 = initial_state(tile.lbm, rho, u, v, w, uvel)
+    R = [tile.lbm.empty_s() for _ in range(4)]
+    tile.lbm.macrovars(*R, f1)
+    tile.lbm.state_import(f1, f2, *R)
+    del f1, f2, R, rho, u, v, w
+
+    def run(n):
+        if world > 1:
+            tile.step(n)
+        else:
+            slabs.step_local([tile], n)
+    run(max(3, a.warmup))
+    torch.cuda.synchronize()
+    steps = a.steps if a.steps != 1000 else 200
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record()
+        run(steps)
+        e1.record()
+        torch.cuda.synchronize()
+    ms = replicas.max_over_ranks(e0.elapsed_time(e1), device="cuda" if world > 1 else "cpu")
+    cells = wl.nx * wl.ny * wl.nz * world
+    plane = tile.lbm.halo_plane_bytes()
+    line = {"metric": "MLUPS of j slabs with the halo exchange after every step", "value":
+            round(cells * steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS", "n_gpus": world, "steps": steps,
+            "warmup": max(3, a.warmup), "ms_per_step": round(ms / steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": a.storage, "data": "synthetic (seeded per tile)",
+            "config": {"workload": "slabs_" + wl.name, "tiles": world, "tile": [wl.nx, wl.ny, wl.nz],
+                       "lattice": "D3Q%d" % wl.nl, "exchange": "nccl p2p" if world > 1 else "one tile, a ring to itself",
+                       "turbulence": "none (the slab tiles carry no inflow-turbulence slice here)",
+                       "l2": "inputs larger than L2"},
+            "halo_bytes_per_step_per_tile": 2 * plane, "clocks": clk.report()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tile.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     a = parse()
+    if a.slabs and a.impl == "ours":
+        return slab_bench(a)
     if a.adjoint_step and a.impl == "ours":
         return adjoint_step_bench(a)
     if a.adjoint and a.impl == "ours":

@@ -278,7 +278,7 @@ void setup_boundaries(lbm_ctx* c) {
     int ko1, koN;
     closed_opts(kb, ko1, koN);
     c->fold_cfg = (ib == 1 && jb == 0 && ko1 != 0);
-    c->fold = c->fold_cfg && !c->halo_j;
+    c->fold = c->fold_cfg;
     c->kopt_lo = ko1;
     c->kopt_hi = koN;
     // m_boundary_i_inflow_kernel.F90:191-193: cos(udir*pi/180), sin(udir*pi/180) in single precision
@@ -447,7 +447,18 @@ int step_one(lbm_ctx* c) {
     } else if (c->fold) {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
+        if (c->halo_j) {
+            // a j-slab tile: pull the stored halo planes, keep the folded boundaries
+            if (!pair_ok(c))
+                return fail(c, LBM_ERR_UNSUPPORTED, "step: a j-slab tile in the folded configuration runs the "
+                                                    "two-cells-per-thread kernel (LBM_KERNEL_PAIR, ihrr = 1, even nx >= 4)");
+            if (c->force)
+                k_step_pair<Q, S, false, true, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            else
+                k_step_pair<Q, S, false, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
+            c->launches++;
+            LBM_LAUNCHED(c, "fused step (pair, j-slab tile)");
+        } else if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
             LBM_TRY(tma_launch<Q, S, true>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
         } else if (pair_ok(c)) {
             if (c->force)
@@ -1124,7 +1135,6 @@ int lbm_set_halo_j(lbm_ctx* c, int32_t on) {
     if (!c) return LBM_ERR_ARG;
     if (c->state != ST_NONE) return fail(c, LBM_ERR_STATE, "set_halo_j: call it before the first import");
     c->halo_j = (on != 0);
-    c->fold = c->fold_cfg && !c->halo_j;
     return LBM_OK;
 }
 
@@ -1137,12 +1147,14 @@ int lbm_halo_plane_bytes(lbm_ctx* c, int64_t* bytes) {
 static int halo_plane(lbm_ctx* c, void* buf, int j, bool unpack) {
     const dim3 grd((unsigned)((c->p.nx + 2 + 127) / 128), (unsigned)(c->p.nz + 2), (unsigned)c->p.nl);
     void* f = c->buf[c->cur];
+    // folded configuration after a step: the x ghosts of every direction are in the compact array
+    const void* xg = (c->fold && c->state == ST_POST) ? c->d_xg[c->cur] : nullptr;
     if (c->elem == 2) {
-        if (unpack) k_halo_plane<uint16_t, true><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j);
-        else k_halo_plane<uint16_t, false><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j);
+        if (unpack) k_halo_plane<uint16_t, true><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, nullptr);
+        else k_halo_plane<uint16_t, false><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, (const uint16_t*)xg);
     } else {
-        if (unpack) k_halo_plane<uint32_t, true><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j);
-        else k_halo_plane<uint32_t, false><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j);
+        if (unpack) k_halo_plane<uint32_t, true><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, nullptr);
+        else k_halo_plane<uint32_t, false><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, (const uint32_t*)xg);
     }
     c->launches++;
     return LBM_OK;

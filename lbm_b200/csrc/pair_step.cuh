@@ -232,10 +232,10 @@ struct PairLoad<Q, S, Q> {
 __device__ __forceinline__ float comp(f2 v, int c) { return c ? v.y : v.x; }
 
 // Everything after the loads of one pair: moments, collision, turbulence slice,
-// solid swap, stores and the edge copy of the folded boundaries.  (Variants that
-// moved the turbulence slice out of this kernel -- a one-cell post-pass, or a
+// solid swap, stores and the edge copy of the folded boundaries (FOLD).  (Variants
+// that moved the turbulence slice out of this kernel -- a one-cell post-pass, or a
 // captured FP32 copy finished by a second kernel -- measured slower on B200.)
-template <int Q, typename S, bool WRAP, bool FORCE = false>
+template <int Q, typename S, bool FOLD, bool FORCE = false>
 __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, const StepArgs& a, long long o, int i,
                                             int j, int k) {
     Moments2 m = moments_rows2<Q>(fp);
@@ -311,7 +311,7 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
         if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
         else *reinterpret_cast<float2*>(qb) = fp[l];
     }
-    if (WRAP && (i == 1 || i + 1 == a.g.nx)) {
+    if (FOLD && (i == 1 || i + 1 == a.g.nx)) {
         // the boundary kernel builds the inflow/outflow ghosts from these, read coalesced
         const long long nyz = (long long)a.g.ny * a.g.nz;
         const int c = (i == 1) ? 0 : 1;
@@ -324,8 +324,11 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
     }
 }
 
-// One pair (i, i+1), i odd, of row (j, k): pull, collide, store.
-template <int Q, typename S, bool WRAP, bool FORCE = false>
+// One pair (i, i+1), i odd, of row (j, k): pull, collide, store.  WRAP: periodic
+// j read through rows ny and 1; FOLD: the folded boundaries follow (edge copy).
+// A j-slab tile in the folded configuration pulls its stored halo planes
+// (WRAP false) and keeps the folded boundaries (FOLD true).
+template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
 __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restrict__ dst, const StepArgs& a, int i, int j,
                                           int k) {
     const long long o = a.g.off(i, j, k);
@@ -337,7 +340,7 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
         const S* pym = (WRAP && j == a.g.ny) ? p0 - wrapd : p0;
         PairLoad<Q, S, 0>::run(fp, p0, pyp, pym, a);
     }
-    pair_update<Q, S, WRAP, FORCE>(fp, dst, a, o, i, j, k);
+    pair_update<Q, S, FOLD, FORCE>(fp, dst, a, o, i, j, k);
 }
 
 #ifndef LBM_PAIR_MIN_BLOCKS
@@ -345,12 +348,12 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 #endif
 // Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
 // ihrr = 1, nx even and Q * dstride < 2^31.
-template <int Q, typename S, bool WRAP, bool FORCE = false>
+template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
 __global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
                                                                         StepArgs a) {
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     if (i > a.g.nx) return;
-    pair_cell<Q, S, WRAP, FORCE>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);
+    pair_cell<Q, S, WRAP, FORCE, FOLD>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);
 }
 
 }  // namespace lbm

@@ -311,16 +311,23 @@ inline long long fold_ghost_cells(const SoaGrid& g) {
 
 // Plane j of a state buffer (every i = 0..nx+1, k = 0..nz+1 and direction) to or
 // from a contiguous array buf[l][k][i]: the halo planes of a j slab.  UNPACK:
-// buf -> buffer.  Grid: x over i, y = k, z = l.
+// buf -> buffer.  xg (packing, folded configuration): the compact x-ghost array
+// of the buffer, which holds every direction of the x ghosts of rows 1..ny (the
+// rows hold only the pulled ones).  Grid: x over i, y = k, z = l.
 template <typename T, bool UNPACK>
-__global__ void __launch_bounds__(128) k_halo_plane(T* buf, T* f, SoaGrid g, int j) {
+__global__ void __launch_bounds__(128) k_halo_plane(T* buf, T* f, SoaGrid g, int j, const T* __restrict__ xg) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > g.nx + 1) return;
     const int k = blockIdx.y, l = blockIdx.z;
     const long long q = ((long long)l * (g.nz + 2) + k) * (g.nx + 2) + i;
     const long long o = (long long)l * g.dstride + g.off(i, j, k);
-    if (UNPACK) f[o] = buf[q];
-    else buf[q] = f[o];
+    if (UNPACK) {
+        f[o] = buf[q];
+    } else {
+        const int Q = (int)gridDim.z;
+        const bool fromxg = xg && (i == 0 || i == g.nx + 1) && k >= 1 && k <= g.nz && j >= 1 && j <= g.ny;
+        buf[q] = fromxg ? xg[xg_index(g, Q, i == 0 ? 0 : 1, l, j, k)] : f[o];
+    }
 }
 
 // The ghost shell of a state buffer to or from a compact array
