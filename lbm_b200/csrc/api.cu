@@ -1145,16 +1145,18 @@ int lbm_halo_plane_bytes(lbm_ctx* c, int64_t* bytes) {
 }
 
 static int halo_plane(lbm_ctx* c, void* buf, int j, bool unpack) {
-    const dim3 grd((unsigned)((c->p.nx + 2 + 127) / 128), (unsigned)(c->p.nz + 2), (unsigned)c->p.nl);
+    const long long n = (long long)c->p.nl * (c->p.nz + 2) * (c->p.nx + 2);
+    const unsigned grd = (unsigned)((n + 255) / 256);
+    const int Q = c->p.nl;
     void* f = c->buf[c->cur];
     // folded configuration after a step: the x ghosts of every direction are in the compact array
     const void* xg = (c->fold && c->state == ST_POST) ? c->d_xg[c->cur] : nullptr;
     if (c->elem == 2) {
-        if (unpack) k_halo_plane<uint16_t, true><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, nullptr);
-        else k_halo_plane<uint16_t, false><<<grd, 128, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, (const uint16_t*)xg);
+        if (unpack) k_halo_plane<uint16_t, true><<<grd, 256, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, Q, nullptr);
+        else k_halo_plane<uint16_t, false><<<grd, 256, 0, c->stream>>>((uint16_t*)buf, (uint16_t*)f, c->sg, j, Q, (const uint16_t*)xg);
     } else {
-        if (unpack) k_halo_plane<uint32_t, true><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, nullptr);
-        else k_halo_plane<uint32_t, false><<<grd, 128, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, (const uint32_t*)xg);
+        if (unpack) k_halo_plane<uint32_t, true><<<grd, 256, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, Q, nullptr);
+        else k_halo_plane<uint32_t, false><<<grd, 256, 0, c->stream>>>((uint32_t*)buf, (uint32_t*)f, c->sg, j, Q, (const uint32_t*)xg);
     }
     c->launches++;
     return LBM_OK;

@@ -313,18 +313,22 @@ inline long long fold_ghost_cells(const SoaGrid& g) {
 // from a contiguous array buf[l][k][i]: the halo planes of a j slab.  UNPACK:
 // buf -> buffer.  xg (packing, folded configuration): the compact x-ghost array
 // of the buffer, which holds every direction of the x ghosts of rows 1..ny (the
-// rows hold only the pulled ones).  Grid: x over i, y = k, z = l.
+// rows hold only the pulled ones).  One thread per element of buf, flat (the
+// plane is 2 KB row segments spread over the whole buffer; more elements per
+// thread measured no faster).
 template <typename T, bool UNPACK>
-__global__ void __launch_bounds__(128) k_halo_plane(T* buf, T* f, SoaGrid g, int j, const T* __restrict__ xg) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > g.nx + 1) return;
-    const int k = blockIdx.y, l = blockIdx.z;
-    const long long q = ((long long)l * (g.nz + 2) + k) * (g.nx + 2) + i;
+__global__ void __launch_bounds__(256) k_halo_plane(T* buf, T* f, SoaGrid g, int j, int Q, const T* __restrict__ xg) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int w = g.nx + 2;
+    const long long n = (long long)Q * (g.nz + 2) * w;
+    if (q >= n) return;
+    const long long r = q / w;
+    const int i = (int)(q - r * w);
+    const int k = (int)(r % (g.nz + 2)), l = (int)(r / (g.nz + 2));
     const long long o = (long long)l * g.dstride + g.off(i, j, k);
     if (UNPACK) {
         f[o] = buf[q];
     } else {
-        const int Q = (int)gridDim.z;
         const bool fromxg = xg && (i == 0 || i == g.nx + 1) && k >= 1 && k <= g.nz && j >= 1 && j <= g.ny;
         buf[q] = fromxg ? xg[xg_index(g, Q, i == 0 ? 0 : 1, l, j, k)] : f[o];
     }
