@@ -99,15 +99,16 @@ def test_tiles_match_tiled_oracle(nl, ntiles, codes):
         compare_to_floor(gpu[r], ref32[r], ref64[r], "tile %d of %d, codes %s" % (r, ntiles, codes))
 
 
-@pytest.mark.parametrize("nl", [19, 27])
-def test_tiles_equal_the_undivided_domain_with_periodic_k(nl):
+@pytest.mark.parametrize("nl,storage", [(19, "f32"), (27, "f32"), (27, "f16")])
+def test_tiles_equal_the_undivided_domain_with_periodic_k(nl, storage):
     """inflow i, periodic j and k: no boundary kernel reads a j ghost between the
-    tile-local j copies and the exchange, so tiles and the whole domain agree."""
+    tile-local j copies and the exchange, so tiles and the whole domain agree
+    (FP16 storage moves 16-bit planes)."""
     from lbm_b200 import Lbm
     wl = W.Workload("slabs", 16, 12, 8, nl, steps=12, ibnd=1, jbnd=0, kbnd=0, noise=3e-3, sphere=(6, 5, 4, 2))
-    tiles = gpu_tiles(wl, 3, wl.steps)
+    tiles = gpu_tiles(wl, 3, wl.steps, storage=storage)
     fA, fB, R, blank, uvel = global_start(wl)
-    L = Lbm(params_of(wl, iturb_pos=3))
+    L = Lbm(params_of(wl, iturb_pos=3, storage=storage))
     L.set_solids(cuda(blank.astype(np.int32)))
     L.set_inflow(cuda(uvel.astype(np.float32)))
     L.state_import(*(cuda(a.astype(np.float32)) for a in (fA, fB, *R)))
