@@ -242,14 +242,14 @@ __global__ void __launch_bounds__(32) k_sadj_xface(float* __restrict__ W, const 
 // step's fused state buffer, offsets f - w, FP32); otherwise it is P itself
 // (the state as imported).  wrap: P has periodic j without stored ghost rows;
 // awrap: the adjoint arrays read their j ghost rows as rows ny and 1 (SoaAdjAcc).
-template <int Q, bool PULL>
-__global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const float* __restrict__ A,
-                                                   const float* __restrict__ P, SoaGrid g, int wrap, int awrap,
-                                                   const uint8_t* __restrict__ solid, CollideParams cp,
-                                                   const float* __restrict__ abl) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
-    if (i > g.nx) return;
+// ROWS: the row is j = 1 or ny, where periodic j wraps (otherwise the wrap
+// adjustments of every address are compiled out).
+template <int Q, bool PULL, bool ROWS>
+__device__ __forceinline__ void sadj_cell(float* __restrict__ W, const float* __restrict__ A,
+                                          const float* __restrict__ P, const SoaGrid& g, int wrap_, int awrap_,
+                                          const uint8_t* __restrict__ solid, const CollideParams& cp,
+                                          const float* __restrict__ abl, int i, int j, int k) {
+    const int wrap = ROWS ? wrap_ : 0, awrap = ROWS ? awrap_ : 0;
     const long long o = g.off(i, j, k);
     float fp[Q], gh[Q];
     if (PULL) {
@@ -304,6 +304,18 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
         W[(long long)l * g.dstride + o] = E + O;
         W[(long long)(l + 1) * g.dstride + o] = E - O;
     }
+}
+
+template <int Q, bool PULL>
+__global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const float* __restrict__ A,
+                                                   const float* __restrict__ P, SoaGrid g, int wrap, int awrap,
+                                                   const uint8_t* __restrict__ solid, CollideParams cp,
+                                                   const float* __restrict__ abl) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    if (j == 1 || j == g.ny) sadj_cell<Q, PULL, true>(W, A, P, g, wrap, awrap, solid, cp, abl, i, j, k);
+    else sadj_cell<Q, PULL, false>(W, A, P, g, wrap, awrap, solid, cp, abl, i, j, k);
 }
 
 // loss seed: A(l, x_p) += d(u, v, w)(x_p)/df_l^T uhat_p at the probe cells, where
