@@ -74,20 +74,29 @@ class Config:
         return (self.nz + 2, self.ny + 2, self.nx + 2)
 
 
-_lib = None
+_libs = {}
+_threads = None
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        path = _build.build()
-        _lib = ctypes.CDLL(path)
-        _lib.orc_set_threads.argtypes = [ctypes.c_int]
-    return _lib
+def lib(contract: bool = False):
+    """The oracle library: separately rounded (default, as the reference's CPU
+    build) or FMA-contracted (contract=True)."""
+    if contract not in _libs:
+        path = _build.build(contract=contract)
+        L = ctypes.CDLL(path)
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        if _threads is not None:
+            L.orc_set_threads(_threads)
+        _libs[contract] = L
+    return _libs[contract]
 
 
 def set_threads(n: int) -> None:
-    lib().orc_set_threads(int(n))
+    global _threads
+    _threads = int(n)
+    lib()
+    for L in _libs.values():
+        L.orc_set_threads(_threads)
 
 
 def _ptr(a):
@@ -98,15 +107,16 @@ def _ptr(a):
 
 
 class Oracle:
-    """Typed front end; ``dtype`` selects the FP32 or FP64 instantiation."""
+    """Typed front end; ``dtype`` selects the FP32 or FP64 instantiation,
+    ``contract`` the FMA-contracted build of the same source."""
 
-    def __init__(self, cfg: Config, dtype=np.float32):
+    def __init__(self, cfg: Config, dtype=np.float32, contract: bool = False):
         self.cfg = cfg
         self.dtype = np.dtype(dtype)
         self.sfx = "f32" if self.dtype == np.float32 else "f64"
         self._p = cfg.c()
         self._pp = ctypes.byref(self._p)
-        self.L = lib()
+        self.L = lib(contract)
 
     def _fn(self, name):
         fn = getattr(self.L, "orc_%s_%s" % (name, self.sfx))

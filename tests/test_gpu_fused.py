@@ -39,11 +39,11 @@ def params_of(wl, **kw):
     return Params(**base)
 
 
-def run_oracle(wl, steps, dtype, iturb, blank, turb):
+def run_oracle(wl, steps, dtype, iturb, blank, turb, contract=False):
     cfg = O.Config(wl.nx, wl.ny, wl.nz, wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=iturb,
                    lsolids=blank is not None, lturb=turb is not None, nrturb=wl.nrturb, kinevisc=wl.kinevisc,
                    smagorinsky=wl.smagorinsky, ampl=wl.ampl)
-    o = O.Oracle(cfg, dtype)
+    o = O.Oracle(cfg, dtype, contract=contract)
     rho, u, v, w = (a.astype(dtype) for a in W.initial_macro(wl))
     uvel = W.inflow_profile(wl, dtype)
     fA, fB = o.zeros_f(), o.zeros_f()
@@ -229,6 +229,14 @@ def test_sphere_200_steps_parity():
     floor = errors(ref32, ref64)
     print("vs oracle FP32:", errs, "vs FP64:", e64, "FP32 floor:", floor)
     assert all(e64[k] <= 1.5 * floor[k] + 5e-8 for k in floor), (e64, floor)
+    # the same oracle built with FMA contraction (as a GPU build contracts): the
+    # GPU is within the bound of both FP32 builds, and contraction alone moves
+    # the FP32 result by less than the FP32 floor
+    ref32c = run_oracle(wl, wl.steps, np.float32, 10, blank, None, contract=True)
+    errs_c = compare(gpu, ref32c, 1e-5, "sphere fused vs FMA-contracted oracle FP32")
+    shift = errors(ref32, ref32c)
+    print("vs FMA-contracted oracle FP32:", errs_c, "contraction shift:", shift)
+    assert all(shift[k] <= floor[k] for k in floor), (shift, floor)
 
 
 def test_f16_storage_error_budget():
