@@ -28,6 +28,7 @@ if ROOT not in sys.path:
 METRIC = "MLUPS & % of HBM roofline: FP16-offset store vs plain FP32 at stated L2 error"
 L2_NOTE = "inputs larger than L2: the two distribution buffers (7.8 GB) exceed the 126 MB L2, no flush needed"
 FALLBACK_HBM_GBS = 6650.0
+NOMINAL_HBM_GBS = 8000.0          # B200 HBM3e, the nominal figure the fraction is also quoted against
 
 
 def parse():
@@ -793,6 +794,7 @@ def main():
                          "traffic": traffic, "peak_kind": hbm_kind,
                          "kernel": key, "kernel_ms": round(k_ms, 4), "kernel_launches": kn,
                          "algorithmic_bytes_per_launch": cells * bl,
+                         "frac_of_nominal_8000_gbs": round(achieved / NOMINAL_HBM_GBS, 4) if achieved else None,
                          "note": "frac of %s HBM copy bandwidth; traffic = ncu dram bytes per launch" % hbm_kind},
             "gpu_launches": launched, "clocks": clk.report(), "status_flags": st}
 
