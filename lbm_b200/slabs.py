@@ -106,11 +106,13 @@ class SlabTile:
     def step(self, n: int = 1, group=None):
         """n steps of this rank's tile with a halo exchange after each (one
         tile per rank of the default or given process group)."""
+        cur = torch.cuda.current_stream()
         for _ in range(n):
             self.lbm.step(1)
             self.pack()
-            self.lbm.stream.synchronize()
+            cur.wait_stream(self.lbm.stream)          # the sends read the packed planes
             exchange(self.send[0], self.send[1], self.recv[0], self.recv[1], self.south, self.north, group)
+            self.lbm.stream.wait_stream(cur)          # the unpack reads what arrived
             self.unpack()
 
     def close(self):
