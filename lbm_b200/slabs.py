@@ -122,14 +122,18 @@ class SlabTile:
 def step_local(tiles: list[SlabTile], n: int = 1):
     """n steps of all tiles of a domain held in one process (one device): each
     tile steps, then the planes move between the tiles' buffers."""
+    cur = torch.cuda.current_stream()
     for _ in range(n):
         for t in tiles:
             t.lbm.step(1)
             t.pack()
+        for t in tiles:
+            cur.wait_stream(t.lbm.stream)
         for t in tiles:
             if t.south is not None:
                 t.recv[0].copy_(tiles[t.south].send[1])
             if t.north is not None:
                 t.recv[1].copy_(tiles[t.north].send[0])
         for t in tiles:
+            t.lbm.stream.wait_stream(cur)
             t.unpack()
