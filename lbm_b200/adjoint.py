@@ -138,10 +138,11 @@ def initial_state(lbm: Lbm, rho, u, v, w, uvel):
 class FusedProbeProblem:
     """The probe-misfit problem of :class:`ProbeProblem` with the forward run made
     by the fused step (the library's default kernels) and the reverse sweep in
-    the state layout (``lbm_state_adjoint_*``).  Checkpoints are the initial
-    (f1, f2) and, every ``checkpoint`` steps after it, a device snapshot of the
-    fused state (``lbm_state_snapshot``).  Each segment is replayed from its
-    checkpoint, each step writing its state buffer into an array of its own
+    the state layout (``lbm_state_adjoint_*``).  Checkpoints are device
+    snapshots of the fused state (``lbm_state_snapshot``) every ``checkpoint``
+    steps, and for the first segment the imported state buffer (the input of
+    step 0) with a snapshot after step 0.  Each segment is replayed from its
+    snapshot, each step writing its state buffer into an array of its own
     (``lbm_step_to``)."""
 
     def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
@@ -173,9 +174,14 @@ class FusedProbeProblem:
         self.ckpt = {}
         self._import(f1, f2)
         for n in range(self.nsteps):
-            if keep and n % self.K == 0:
-                self.ckpt[n] = (f1.clone(), f2.clone()) if n == 0 else L.snapshot()
+            if keep and n % self.K == 0 and n > 0:
+                self.ckpt[n] = L.snapshot()
+            if keep and n == 0:
+                pre = L.state_scratch()
+                L.state_copy(pre)            # the imported f1: the input of step 0
             L.step(1)
+            if keep and n == 0:
+                self.ckpt[0] = (pre, L.snapshot())   # and the state after step 0
         R = [L.empty_s() for _ in range(4)]
         L.get_macro(*R)
         return torch.stack([R[q].reshape(-1)[self.pidx] for q in (1, 2, 3)], dim=1)
@@ -208,30 +214,30 @@ class FusedProbeProblem:
         R.set_inflow(self.uvel)
         nsets = 2 if overlap else 1
         sets = [[L.state_scratch() for _ in range(self.K)] for _ in range(nsets)]
-        firsts = [L.state_scratch() for _ in range(nsets)]
         released = [None] * nsets            # event: the adjoint is done with a set
 
         def replay(q):
+            """The states of segment q: P[n - s] after step n, and the input of step s."""
             s, b = segs[q], q % nsets
             e = min(s + self.K, self.nsteps)
+            P = list(sets[b][:e - s])
             with torch.cuda.stream(rep):
                 if released[b] is not None:
                     rep.wait_event(released[b])
                 if s == 0:
-                    Rm = [R.empty_s() for _ in range(4)]
-                    f1, f2 = self.ckpt[0]
-                    R.macrovars(*Rm, f1)
-                    R.state_import(f1, f2, *Rm)
-                    R.state_copy(firsts[b])  # the imported f1: input of step 0
-                    first = firsts[b]
+                    first, after0 = self.ckpt[0]  # the imported f1 (a step-0 input, not pulled) and the state after step 0
+                    P[0] = after0
+                    R.restore(after0)
+                    start = 1
                 else:
                     first = self.ckpt[s]     # the state after step s - 1, which step s pulls from
                     R.restore(first)
-                for n in range(s, e):
-                    R.step_to(sets[b][n - s])  # the step writes its state into the array
+                    start = s
+                for n in range(start, e):
+                    R.step_to(P[n - s])      # the step writes its state into the array
                 ready = torch.cuda.Event()
                 ready.record(rep)
-            return first, ready
+            return first, P, ready
 
         # The adjoint steps of segment q are enqueued before the replay of q + 1:
         # restoring a snapshot reads its header on the host, which waits for the
@@ -240,9 +246,8 @@ class FusedProbeProblem:
         for q, s in enumerate(segs):
             b = q % nsets
             e = min(s + self.K, self.nsteps)
-            first, ready = pending
+            first, P, ready = pending
             main.wait_event(ready)
-            P = sets[b]
             with torch.cuda.stream(main):
                 if e == self.nsteps:
                     L.state_adjoint_seed(A, P[e - s - 1], self.probes_dev, uhat_probes.float())
@@ -258,7 +263,7 @@ class FusedProbeProblem:
         g = L.empty_f()
         L.state_adjoint_export(g, A)
         main.synchronize()
-        del sets, firsts
+        del sets
         return g, uvel_h
 
     def close(self):

@@ -346,16 +346,25 @@ __global__ void k_sadj_seed(float* A, const float* __restrict__ P, SoaGrid g, in
 }
 
 // a state-layout adjoint to the reference layout (all cells, no weights: adjoints of
-// f and of f - w are the same)
+// f and of f - w are the same).  A block of 128 cells of one row is staged
+// through shared memory, so both the reads (per direction, along i) and the
+// writes (l fastest) are coalesced.  Grid: x over i in blocks of 128, y = j, z = k.
 template <int Q>
-__global__ void k_sadj_export(float* __restrict__ ref, const float* __restrict__ A, SoaGrid g) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_sadj_export(float* __restrict__ ref, const float* __restrict__ A, SoaGrid g) {
+    __shared__ float sm[128 * Q];
+    const int i0 = blockIdx.x * 128;
     const int j = blockIdx.y, k = blockIdx.z;
-    if (i > g.nx + 1) return;
-    const long long c = (long long)i + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k);
-    const long long o = g.off(i, j, k);
+    const int n = min(128, g.nx + 2 - i0);
+    if (n <= 0) return;
+    const int t = threadIdx.x;
+    if (t < n) {
+        const long long o = g.off(i0 + t, j, k);
 #pragma unroll
-    for (int l = 0; l < Q; ++l) ref[c * Q + l] = A[(long long)l * g.dstride + o];
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = A[(long long)l * g.dstride + o];
+    }
+    __syncthreads();
+    const long long base = ((long long)i0 + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k)) * Q;
+    for (int e = t; e < n * Q; e += blockDim.x) ref[base + e] = sm[e];
 }
 
 }  // namespace lbm
