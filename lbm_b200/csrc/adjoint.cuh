@@ -313,43 +313,100 @@ __global__ void __launch_bounds__(128) k_ref_macrovars_adj(float* fh, const floa
     tile_store<Q>(sg, fh, g.cell(i0, j, k), n);
 }
 
-// drift adjoint, gather form: fh_in(l, y) += fh_out(l, y + c_l) where y + c_l is
-// an interior cell.  A thread per (l, i) of a row y over the ghost-inclusive grid.
-__global__ void k_ref_drift_adj(float* fh_in, const float* fh_out, RefGrid g) {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y, k = blockIdx.z;
-    const int nl = g.nl;
-    if (idx >= nl * (g.nx + 2)) return;
-    const int l = idx % nl, i = idx / nl;
-    const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
-    if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) return;
-    fh_in[g.cell(i, j, k) * nl + l] += fh_out[g.cell(ti, tj, tk) * nl + l];
+// Per-direction tables of the drift adjoints, in shared memory: a constant read
+// indexed by l would serialise over the different directions of a warp.
+template <int Q>
+struct DriftTab {
+    int cx[Q], cy[Q], cz[Q];
+    long long d[Q];   // cell distance cx + (nx+2) cy + (nx+2)(ny+2) cz
+};
+template <int Q>
+__device__ __forceinline__ void drift_tab(DriftTab<Q>& t, const RefGrid& g) {
+    if (threadIdx.x < Q) {
+        const int l = threadIdx.x;
+        t.cx[l] = lat_cx(l);
+        t.cy[l] = lat_cy(l);
+        t.cz[l] = lat_cz(l);
+        t.d[l] = lat_cx(l) + (long long)lat_cy(l) * (g.nx + 2) + (long long)lat_cz(l) * (g.nx + 2) * (g.ny + 2);
+    }
+    __syncthreads();
+}
+#define DRIFT_ADJ_ILP 4
+
+// drift adjoint: fh_in(l, y) += fh_out(l, y + c_l) for y + c_l interior (the
+// transpose of the pull).  One block per row (j,k) of the ghost-inclusive grid,
+// looping over its (nx+2)*Q entries, DRIFT_ADJ_ILP loads in flight per thread.
+template <int Q>
+__global__ void __launch_bounds__(256) k_ref_drift_adj(float* __restrict__ fh_in, const float* __restrict__ fh_out,
+                                                       RefGrid g) {
+    __shared__ DriftTab<Q> t;
+    drift_tab<Q>(t, g);
+    const int j = blockIdx.x, k = blockIdx.y;
+    const long long c0 = g.cell(0, j, k);
+    const int n = Q * (g.nx + 2);
+    for (int e0 = threadIdx.x; e0 < n; e0 += blockDim.x * DRIFT_ADJ_ILP) {
+        float val[DRIFT_ADJ_ILP];
+        bool ok[DRIFT_ADJ_ILP];
+#pragma unroll
+        for (int u = 0; u < DRIFT_ADJ_ILP; ++u) {
+            const int e = e0 + u * blockDim.x;
+            ok[u] = false;
+            if (e >= n) continue;
+            const int l = e % Q, i = e / Q;
+            const int ti = i + t.cx[l], tj = j + t.cy[l], tk = k + t.cz[l];
+            if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) continue;
+            ok[u] = true;
+            val[u] = fh_in[c0 * Q + e] + fh_out[(c0 + i + t.d[l]) * Q + l];
+        }
+#pragma unroll
+        for (int u = 0; u < DRIFT_ADJ_ILP; ++u)
+            if (ok[u]) fh_in[c0 * Q + e0 + u * blockDim.x] = val[u];
+    }
 }
 
 // drift adjoint preceded by the adjoint of the macrovars call that followed the
 // drift: fh_in(l, y) += fh_out(l, x) + d(rho, u)(x)/df_l^T (rhoh, uh, vh, wh)(x)
 // for x = y + c_l interior, where rho(x), u(x) are the macrovars outputs.  The
-// macrovars adjoints are taken at interior cells only.
+// macrovars adjoints are taken at interior cells only.  Layout and loop as
+// k_ref_drift_adj.
 template <int Q>
-__global__ void __launch_bounds__(256) k_ref_macro_drift_adj(float* fh_in, const float* fh_out, const float* rhoh,
-                                                             const float* uh, const float* vh, const float* wh,
-                                                             const float* rho, const float* u, const float* v,
-                                                             const float* w, RefGrid g) {
-    // one block per row (j,k) of the ghost-inclusive grid, looping over its (nx+2)*Q entries
+__global__ void __launch_bounds__(256) k_ref_macro_drift_adj(float* __restrict__ fh_in,
+                                                             const float* __restrict__ fh_out,
+                                                             const float* __restrict__ rhoh,
+                                                             const float* __restrict__ uh,
+                                                             const float* __restrict__ vh,
+                                                             const float* __restrict__ wh,
+                                                             const float* __restrict__ rho,
+                                                             const float* __restrict__ u,
+                                                             const float* __restrict__ v,
+                                                             const float* __restrict__ w, RefGrid g) {
+    __shared__ DriftTab<Q> t;
+    drift_tab<Q>(t, g);
     const int j = blockIdx.x, k = blockIdx.y;
-    float* row = fh_in + g.cell(0, j, k) * Q;
+    const long long c0 = g.cell(0, j, k);
     const int n = Q * (g.nx + 2);
-    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-        const int l = idx % Q, i = idx / Q;
-        const int ti = i + c_cx[l], tj = j + c_cy[l], tk = k + c_cz[l];
-        if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) continue;
-        const long long x = g.cell(ti, tj, tk);
-        const float inv = 1.0f / __ldg(rho + x);
-        const float ux = __ldg(u + x), uy = __ldg(v + x), uz = __ldg(w + x);
-        const float ax = __ldg(uh + x) * inv, ay = __ldg(vh + x) * inv, az = __ldg(wh + x) * inv;
-        const float m =
-            __ldg(rhoh + x) + ax * ((float)c_cx[l] - ux) + ay * ((float)c_cy[l] - uy) + az * ((float)c_cz[l] - uz);
-        row[idx] += fh_out[x * Q + l] + m;
+    for (int e0 = threadIdx.x; e0 < n; e0 += blockDim.x * DRIFT_ADJ_ILP) {
+        float val[DRIFT_ADJ_ILP];
+        bool ok[DRIFT_ADJ_ILP];
+#pragma unroll
+        for (int q = 0; q < DRIFT_ADJ_ILP; ++q) {
+            const int e = e0 + q * blockDim.x;
+            ok[q] = false;
+            if (e >= n) continue;
+            const int l = e % Q, i = e / Q;
+            const int cx = t.cx[l], cy = t.cy[l], cz = t.cz[l];
+            const int ti = i + cx, tj = j + cy, tk = k + cz;
+            if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) continue;
+            ok[q] = true;
+            const long long x = c0 + i + t.d[l];
+            const float inv = 1.0f / rho[x];
+            const float ax = uh[x] * inv, ay = vh[x] * inv, az = wh[x] * inv;
+            const float m = rhoh[x] + ax * ((float)cx - u[x]) + ay * ((float)cy - v[x]) + az * ((float)cz - w[x]);
+            val[q] = fh_in[c0 * Q + e] + (fh_out[x * Q + l] + m);
+        }
+#pragma unroll
+        for (int q = 0; q < DRIFT_ADJ_ILP; ++q)
+            if (ok[q]) fh_in[c0 * Q + e0 + q * blockDim.x] = val[q];
     }
 }
 

@@ -96,9 +96,9 @@ int lbm_drift_adj(lbm_ctx* c, float* fhat_in, float* fhat_out) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, fhat_in); NEED(c, fhat_out);
     if (fhat_in == fhat_out) return fail(c, LBM_ERR_ARG, "drift_adj: the two adjoint arrays must be distinct");
-    const int nl = c->p.nl;
-    k_ref_drift_adj<<<dim3((nl * (c->p.nx + 2) + 127) / 128, c->p.ny + 2, c->p.nz + 2), 128, 0, c->stream>>>(
-        fhat_in, fhat_out, c->rg);
+    const dim3 grd(c->p.ny + 2, c->p.nz + 2);
+    if (c->p.nl == 27) k_ref_drift_adj<27><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, c->rg);
+    else k_ref_drift_adj<19><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, c->rg);
     k_ref_zero_interior<<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(fhat_out, c->rg);
     c->launches += 2;
     LBM_LAUNCHED(c, "drift adjoint");

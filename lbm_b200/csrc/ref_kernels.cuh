@@ -131,16 +131,37 @@ __global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, cons
 }
 
 // drift: f(l,i,j,k) = feq(l,i-cx,j-cy,k-cz) over interior cells; a thread per
-// (l,i) of a row, as m_drift_kernel.F90:62-84 flattens it
+// (l,i) of a row, as m_drift_kernel.F90:62-84 flattens it.  The source of
+// element e = (i-1) Q + l of a row is e minus the direction's distance Q d_l,
+// d_l = cx + (nx+2) cy + (nx+2)(ny+2) cz, taken from shared memory (a constant
+// read would serialise over the different l of a warp).  Each thread keeps
+// DRIFT_ILP loads in flight before its stores.
+#define DRIFT_ILP 4
 template <int Q>
-__global__ void __launch_bounds__(256) k_ref_drift(float* f, const float* feq, RefGrid g) {
+__global__ void __launch_bounds__(256) k_ref_drift(float* __restrict__ f, const float* __restrict__ feq, RefGrid g) {
     // one block per interior row (j,k), looping over its nx*Q outputs
+    __shared__ long long sd[Q];
+    if (threadIdx.x < Q) {
+        const int l = threadIdx.x;
+        sd[l] = (long long)Q * (lat_cx(l) + (long long)lat_cy(l) * (g.nx + 2) +
+                                (long long)lat_cz(l) * (g.nx + 2) * (g.ny + 2));
+    }
+    __syncthreads();
     const int j = blockIdx.x + 1, k = blockIdx.y + 1;
-    float* out = f + g.cell(1, j, k) * Q;
+    const long long base = g.cell(1, j, k) * Q;
     const int n = Q * g.nx;
-    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-        const int l = idx % Q, i = idx / Q + 1;
-        out[idx] = feq[g.cell(i - c_cx[l], j - c_cy[l], k - c_cz[l]) * Q + l];
+    for (int e0 = threadIdx.x; e0 < n; e0 += blockDim.x * DRIFT_ILP) {
+        float v[DRIFT_ILP];
+#pragma unroll
+        for (int u = 0; u < DRIFT_ILP; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < n) v[u] = feq[base + e - sd[e % Q]];
+        }
+#pragma unroll
+        for (int u = 0; u < DRIFT_ILP; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < n) f[base + e] = v[u];
+        }
     }
 }
 
