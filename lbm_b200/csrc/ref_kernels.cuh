@@ -67,15 +67,31 @@ __device__ __forceinline__ void regularized(float (&out)[Q], const Moments& m, f
 }
 
 // Row-chunk staging: cells [i0, i0+n) of row (j,k), n <= 128.
+#define TILE_ILP 8
 template <int Q>
-__device__ __forceinline__ void tile_load(float* sm, const float* f, long long cell0, int n) {
-    const long long base = cell0 * Q;
-    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) sm[e] = f[base + e];
+__device__ __forceinline__ void tile_load(float* __restrict__ sm, const float* __restrict__ f, long long cell0, int n) {
+    // TILE_ILP independent loads in flight per thread before their shared-memory stores
+    const float* src = f + cell0 * Q;
+    const int m = n * Q, step = blockDim.x * TILE_ILP;
+    for (int e0 = threadIdx.x; e0 < m; e0 += step) {
+        float v[TILE_ILP];
+#pragma unroll
+        for (int u = 0; u < TILE_ILP; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < m) v[u] = src[e];
+        }
+#pragma unroll
+        for (int u = 0; u < TILE_ILP; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < m) sm[e] = v[u];
+        }
+    }
 }
 template <int Q>
-__device__ __forceinline__ void tile_store(const float* sm, float* f, long long cell0, int n) {
-    const long long base = cell0 * Q;
-    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) f[base + e] = sm[e];
+__device__ __forceinline__ void tile_store(const float* __restrict__ sm, float* __restrict__ f, long long cell0, int n) {
+    float* dst = f + cell0 * Q;
+    const int m = n * Q;
+    for (int e = threadIdx.x; e < m; e += blockDim.x) dst[e] = sm[e];
 }
 
 // fequil3: feq on interior cells (m_fequil3_kernel.F90:7-123)
