@@ -561,7 +561,21 @@ __global__ void __launch_bounds__(128) k_import(const float* __restrict__ ref, S
     const int n = min(128, g.nx + 2 - i0);
     if (n <= 0) return;
     const long long base = ((long long)i0 + (long long)(g.nx + 2) * ((long long)j + (long long)(g.ny + 2) * k)) * Q;
-    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) sm[e] = ref[base + e];
+    // eight independent loads in flight per thread before their shared-memory stores
+    const int m = n * Q;
+    for (int e0 = threadIdx.x; e0 < m; e0 += blockDim.x * 8) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < m) v[u] = ref[base + e];
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < m) sm[e] = v[u];
+        }
+    }
     __syncthreads();
     const int t = threadIdx.x;
     if (t < n) {
