@@ -244,6 +244,28 @@ def test_autograd_function_gives_the_sweep_gradient():
     pb.close()
 
 
+def test_autograd_function_with_the_state_layout_sweep():
+    """The same torch.autograd wrapper around the fused-forward problem: its
+    gradient is the state-layout sweep's (f1 bit for bit)."""
+    from tests.adjoint_harness import probe_loss
+    wl = CASE.with_(steps=6)
+    pb, f1, f2, uvel = problem(wl, 4)
+    target = pb.forward(f1, f2, uvel + cuda(W.inflow_perturbation(wl.nz, 3, 5e-3)), keep=False)
+    pb.close()
+    fb = fused_problem(wl, 4, None)
+    x1 = f1.clone().requires_grad_(True)
+    xu = uvel.clone().requires_grad_(True)
+    loss = probe_loss(x1, xu, f2, fb, target)
+    g1, gu = torch.autograd.grad(loss, (x1, xu))
+    u = fb.forward(f1, f2, uvel)
+    r1, ru = fb.backward((2.0 * (u.double() - target.double())).float())
+    assert torch.equal(g1, r1)
+    # uvelhat is summed with atomics, whose order may differ between two sweeps
+    assert float((gu - ru).abs().max()) <= 1e-6 * float(ru.abs().max()) + 1e-12
+    assert float(loss.detach()) > 0 and float(g1.abs().sum()) > 0
+    fb.close()
+
+
 def test_fused_adjoints_equal_the_chained_ones():
     """macrovars_drift_adj == macrovars_adj then drift_adj (macrovars adjoints at
     interior cells); postcoll_adj with blanking == solids then postcoll_adj."""
