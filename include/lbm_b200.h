@@ -176,8 +176,11 @@ int lbm_step(lbm_ctx* ctx, int32_t nsteps);
  * reference's MPI tiling (m_mpi_decomp_init.F90:123-134, m_mpi_halo_exchange_j.F90:3-121).
  * A tile is a context whose ny is the tile's rows; lbm_set_halo_j(ctx, 1), before
  * the first import, makes it keep stored j ghost planes that the caller fills
- * (the step reads them instead of wrapping j, the folded boundary path is off).
- * The boundary conditions of a tile run as in the reference, tile by tile; after
+ * (the step reads them instead of wrapping j).  The boundary conditions of a
+ * tile run as in the reference, tile by tile, whose periodic j copies are
+ * tile-local; in the folded configuration that is the folded boundary kernel
+ * wrapping j within the tile, which needs the two-cells-per-thread kernel
+ * (LBM_KERNEL_PAIR, ihrr = 1, even nx >= 4).  After
  * each lbm_step the caller packs planes j = 1 and j = ny of the current state
  * (all i = 0..nx+1, k = 0..nz+1 and directions; lbm_halo_plane_bytes each),
  * sends them to the south and north neighbours, and unpacks what it receives
