@@ -364,26 +364,39 @@ __global__ void __launch_bounds__(256) k_ref_drift_adj(float* __restrict__ fh_in
     }
 }
 
+// The macrovars adjoint at a cell x, as four terms: with a = (uh, vh, wh) / rho,
+// d(rho, u)/df_l^T (rhoh, uh, vh, wh) = (rhoh - a.u) + a.c_l.  One thread per
+// interior cell; T is [4][cells of the ghost-inclusive grid].
+__global__ void __launch_bounds__(256) k_ref_macro_adj_terms(float* __restrict__ T, const float* __restrict__ rhoh,
+                                                             const float* __restrict__ uh, const float* __restrict__ vh,
+                                                             const float* __restrict__ wh, const float* __restrict__ rho,
+                                                             const float* __restrict__ u, const float* __restrict__ v,
+                                                             const float* __restrict__ w, RefGrid g) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y + 1, k = blockIdx.z + 1;
+    if (i > g.nx) return;
+    const long long x = g.cell(i, j, k), n = g.ncell();
+    const float inv = 1.0f / rho[x];
+    const float ax = uh[x] * inv, ay = vh[x] * inv, az = wh[x] * inv;
+    T[x] = rhoh[x] - (ax * u[x] + ay * v[x] + az * w[x]);
+    T[n + x] = ax;
+    T[2 * n + x] = ay;
+    T[3 * n + x] = az;
+}
+
 // drift adjoint preceded by the adjoint of the macrovars call that followed the
 // drift: fh_in(l, y) += fh_out(l, x) + d(rho, u)(x)/df_l^T (rhoh, uh, vh, wh)(x)
-// for x = y + c_l interior, where rho(x), u(x) are the macrovars outputs.  The
-// macrovars adjoints are taken at interior cells only.  Layout and loop as
-// k_ref_drift_adj.
+// for x = y + c_l interior, where rho(x), u(x) are the macrovars outputs and T
+// holds the four terms of k_ref_macro_adj_terms.  The macrovars adjoints are
+// taken at interior cells only.  Layout and loop as k_ref_drift_adj.
 template <int Q>
 __global__ void __launch_bounds__(256) k_ref_macro_drift_adj(float* __restrict__ fh_in,
                                                              const float* __restrict__ fh_out,
-                                                             const float* __restrict__ rhoh,
-                                                             const float* __restrict__ uh,
-                                                             const float* __restrict__ vh,
-                                                             const float* __restrict__ wh,
-                                                             const float* __restrict__ rho,
-                                                             const float* __restrict__ u,
-                                                             const float* __restrict__ v,
-                                                             const float* __restrict__ w, RefGrid g) {
+                                                             const float* __restrict__ T, RefGrid g) {
     __shared__ DriftTab<Q> t;
     drift_tab<Q>(t, g);
     const int j = blockIdx.x, k = blockIdx.y;
-    const long long c0 = g.cell(0, j, k);
+    const long long c0 = g.cell(0, j, k), nc = g.ncell();
     const int n = Q * (g.nx + 2);
     for (int e0 = threadIdx.x; e0 < n; e0 += blockDim.x * DRIFT_ADJ_ILP) {
         float val[DRIFT_ADJ_ILP];
@@ -399,9 +412,7 @@ __global__ void __launch_bounds__(256) k_ref_macro_drift_adj(float* __restrict__
             if (ti < 1 || ti > g.nx || tj < 1 || tj > g.ny || tk < 1 || tk > g.nz) continue;
             ok[q] = true;
             const long long x = c0 + i + t.d[l];
-            const float inv = 1.0f / rho[x];
-            const float ax = uh[x] * inv, ay = vh[x] * inv, az = wh[x] * inv;
-            const float m = rhoh[x] + ax * ((float)cx - u[x]) + ay * ((float)cy - v[x]) + az * ((float)cz - w[x]);
+            const float m = T[x] + (T[nc + x] * (float)cx + T[2 * nc + x] * (float)cy + T[3 * nc + x] * (float)cz);
             val[q] = fh_in[c0 * Q + e] + (fh_out[x * Q + l] + m);
         }
 #pragma unroll

@@ -113,15 +113,16 @@ int lbm_macrovars_drift_adj(lbm_ctx* c, float* fhat_in, float* fhat_out, const f
     NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
     if (fhat_in == fhat_out) return fail(c, LBM_ERR_ARG, "macrovars_drift_adj: the two adjoint arrays must be distinct");
     const int nl = c->p.nl;
+    if (!c->d_adj_terms)
+        LBM_TRY(cuda_check(c, cudaMalloc(&c->d_adj_terms, (size_t)4 * c->rg.ncell() * sizeof(float)),
+                           "cudaMalloc(macrovars adjoint terms)"));
+    k_ref_macro_adj_terms<<<dim3((c->p.nx + 255) / 256, c->p.ny, c->p.nz), 256, 0, c->stream>>>(
+        c->d_adj_terms, rhohat, uhat, vhat, what, rho, u, v, w, c->rg);
     const dim3 grd(c->p.ny + 2, c->p.nz + 2);
-    if (nl == 27)
-        k_ref_macro_drift_adj<27><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w,
-                                                             c->rg);
-    else
-        k_ref_macro_drift_adj<19><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, rhohat, uhat, vhat, what, rho, u, v, w,
-                                                             c->rg);
+    if (nl == 27) k_ref_macro_drift_adj<27><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, c->d_adj_terms, c->rg);
+    else k_ref_macro_drift_adj<19><<<grd, 256, 0, c->stream>>>(fhat_in, fhat_out, c->d_adj_terms, c->rg);
     k_ref_zero_interior<<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(fhat_out, c->rg);
-    c->launches += 2;
+    c->launches += 3;
     LBM_LAUNCHED(c, "macrovars + drift adjoint");
     return LBM_OK;
 }

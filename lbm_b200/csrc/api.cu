@@ -74,6 +74,7 @@ struct lbm_ctx {
     float* d_abl = nullptr;       // ablvisc(nz), zero unless set
     int* d_it = nullptr;          // number of the step being computed
     int* d_status = nullptr;
+    float* d_adj_terms = nullptr; // 4 x cells: the macrovars adjoint terms of lbm_macrovars_drift_adj (allocated on first use)
     double* d_partial = nullptr;  // FP64 block partials of the conservation sums (scratch)
     double* d_sum = nullptr;      // their total (4 doubles)
     int it = 0;
@@ -694,6 +695,7 @@ int lbm_destroy(lbm_ctx* c) {
     cudaFree(c->d_edge);
     for (int b = 0; b < 2; ++b) cudaFree(c->d_xg[b]);
     cudaFree(c->d_abl);
+    cudaFree(c->d_adj_terms);
     cudaFree(c->d_it);
     cudaFree(c->d_status);
     cudaFree(c->d_partial);
