@@ -298,5 +298,65 @@ module lbm_b200_iface
          integer(c_int32_t)        :: variant
          real(c_float)             :: ms_per_step(*)
       end function
+      integer(c_int) function lbm_ensemble_size(ens, nmembers) bind(C, name="lbm_ensemble_size")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value  :: ens
+         integer(c_int32_t)  :: nmembers
+      end function
+      integer(c_int) function lbm_ensemble_set_variant(ens, variant) bind(C, name="lbm_ensemble_set_variant")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: variant
+      end function
+      integer(c_int) function lbm_ensemble_set_graph(ens, graph_steps) bind(C, name="lbm_ensemble_set_graph")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: graph_steps
+      end function
+      type(c_ptr) function lbm_ensemble_last_error(ens) bind(C, name="lbm_ensemble_last_error")
+         import :: c_ptr
+         type(c_ptr), value :: ens            ! C string (c_f_pointer to read it); c_null_ptr: the last failed create
+      end function
+      ! ---- conservation, step counter, instrumentation ----
+      integer(c_int) function lbm_abi_version() bind(C, name="lbm_abi_version")
+         import :: c_int
+      end function
+      integer(c_int) function lbm_get_step(ctx, it) bind(C, name="lbm_get_step")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value  :: ctx
+         integer(c_int32_t)  :: it
+      end function
+      integer(c_int) function lbm_mass_momentum(ctx, f, out) bind(C, name="lbm_mass_momentum")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, out      ! out: 4 doubles on the device
+      end function
+      integer(c_int) function lbm_mass_momentum_noalloc(f, nx, ny, nz, nl, out, stream) &
+            bind(C, name="lbm_mass_momentum_noalloc")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: f, out, stream
+         integer(c_int32_t), value :: nx, ny, nz, nl
+      end function
+      integer(c_int) function lbm_conservation(ctx, out_host) bind(C, name="lbm_conservation")
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value :: ctx
+         real(c_double)     :: out_host(4)      ! mass, x, y, z momentum of the fused state
+      end function
+      integer(c_int) function lbm_launch_count(ctx, n) bind(C, name="lbm_launch_count")
+         import :: c_ptr, c_int, c_int64_t
+         type(c_ptr), value  :: ctx
+         integer(c_int64_t)  :: n
+      end function
+      integer(c_int) function lbm_profile(ctx, enable) bind(C, name="lbm_profile")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ctx
+         integer(c_int32_t), value :: enable
+      end function
+      integer(c_int) function lbm_profile_read(ctx, step_kernel_ms, step_kernel_launches) &
+            bind(C, name="lbm_profile_read")
+         import :: c_ptr, c_int, c_int64_t, c_double
+         type(c_ptr), value  :: ctx
+         real(c_double)      :: step_kernel_ms
+         integer(c_int64_t)  :: step_kernel_launches
+      end function
    end interface
 end module lbm_b200_iface

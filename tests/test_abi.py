@@ -45,6 +45,16 @@ def test_bindings_cover_header():
     assert set(header_functions()) == bound
 
 
+def test_fortran_module_binds_every_header_function():
+    """include/lbm_b200_iface.F90 has an interface (bind(C, name=...)) for every
+    entry point of the header, so a Fortran driver can call all of them."""
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(_lib.LIB_PATH), "..", "include", "lbm_b200_iface.F90")).read()
+    bound = set(re.findall(r'bind\(C,\s*name="(lbm_[a-z0-9_]+)"\)', src))
+    assert set(header_functions()) <= bound, sorted(set(header_functions()) - bound)
+
+
 def test_library_does_not_link_the_oracle(lib):
     out = subprocess.run(["nm", "-D", _lib.LIB_PATH], capture_output=True, text=True, check=True).stdout
     assert "orc_" not in out
