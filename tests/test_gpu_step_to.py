@@ -119,4 +119,14 @@ def test_snapshot_refusals():
     with pytest.raises(LbmError, match="parameters"):
         o.lbm.restore(other)
     o.close()
+    # same grid, FP16 storage: a snapshot of the FP32 state does not restore there
+    h = start(wl, "f16", blank=False)
+    other = torch.zeros((h.lbm.snapshot_bytes() + 3) // 4, device="cuda")
+    n = min(other.numel(), snap.numel())
+    other[:n] = snap[:n]
+    with pytest.raises(LbmError, match="parameters"):
+        h.lbm.restore(other)
+    with pytest.raises(LbmError, match="aligned"):
+        s.lbm._call("lbm_state_restore", snap.data_ptr() + 4)
+    h.close()
     s.close()
