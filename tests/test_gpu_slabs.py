@@ -126,6 +126,21 @@ def test_tiles_equal_the_undivided_domain_with_periodic_k(nl, storage):
             assert np.array_equal(a[1:-1, 1:-1, 1:-1], b[1:-1, rows, 1:-1]), r
 
 
+@pytest.mark.parametrize("nl", [19, 27])
+def test_fp16_tiles_in_the_folded_configuration(nl):
+    """FP16-offset storage through the folded tiles (16-bit planes, x ghosts packed
+    from the compact arrays): within the FP16 error budget of the FP32 tiles."""
+    from tests.conftest import rel_l2
+    wl = W.Workload("slabs", 16, 12, 8, nl, steps=10, ibnd=1, jbnd=0, kbnd=12, noise=3e-3, sphere=(6, 5, 4, 2))
+    t32 = gpu_tiles(wl, 2, wl.steps, storage="f32")
+    t16 = gpu_tiles(wl, 2, wl.steps, storage="f16")
+    s = (slice(1, -1),) * 3
+    for a, b in zip(t16, t32):
+        assert np.all(np.isfinite(a[0]))
+        assert rel_l2(a[2][s], b[2][s]) < 1e-4                                          # rho
+        assert rel_l2(np.stack(a[3:])[(slice(None),) + s], np.stack(b[3:])[(slice(None),) + s]) < 1e-3   # u
+
+
 def test_halo_switch_refusals():
     from lbm_b200 import Lbm, LbmError
     wl = W.Workload("slabs", 16, 12, 8, 19, steps=2)
