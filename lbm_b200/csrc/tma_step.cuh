@@ -10,7 +10,7 @@
 // at fixed offsets instead of forming Q global addresses.
 //
 // Waits are bounded: a stage that does not complete within the iteration limit
-// sets LBM_STATUS_TIMEOUT and the CTA stops.  No copy uses cluster multicast.
+// sets LBM_STATUS_TIMEOUT and the CTA stops.  Every copy lands in the issuing CTA's own shared memory only.
 #pragma once
 
 #include "state_kernels.cuh"
@@ -39,7 +39,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// 1-D bulk copy global -> this CTA's shared memory, completing on bar (no multicast)
+// 1-D bulk copy global -> this CTA's shared memory, completing on bar (this CTA only)
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
