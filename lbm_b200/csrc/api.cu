@@ -384,10 +384,11 @@ StepArgs step_args(lbm_ctx* c) {
         const long long plane = (long long)g.pitch * (g.ny + 2);
         for (int l = 0; l < c->p.nl; ++l) {
             const long long d = lat_cx(l) + (long long)lat_cy(l) * g.pitch + (long long)lat_cz(l) * plane;
-            a.poff[l] = (int)((long long)l * g.dstride - d);
-            a.soff[l] = (int)((long long)l * g.dstride);
-            a.poffb[l] = (long long)a.poff[l] * (long long)c->elem;
-            a.soffb[l] = (long long)a.soff[l] * (long long)c->elem;
+            const long long po = (long long)l * g.dstride - d, so = (long long)l * g.dstride;
+            a.poff[l] = (int)po;   // read only when the state fits 32-bit offsets (idx32)
+            a.soff[l] = (int)so;
+            a.poffb[l] = po * (long long)c->elem;
+            a.soffb[l] = so * (long long)c->elem;
         }
     }
     return a;
@@ -421,8 +422,9 @@ void launch_gather_xg(lbm_ctx* c, int b) {
     c->launches++;
 }
 
-// the two-cells-per-thread kernel (pair_step.cuh) covers the regularized collision on even nx
-bool pair_shape_ok(const lbm_ctx* c) { return c->idx32 && c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
+// the two-cells-per-thread kernel (pair_step.cuh) covers the regularized collision on even nx, at any
+// state size (64-bit byte offsets)
+bool pair_shape_ok(const lbm_ctx* c) { return c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
 bool pair_ok(const lbm_ctx* c) { return c->kernel == LBM_KERNEL_PAIR && pair_shape_ok(c); }
 dim3 pair_grid(const lbm_ctx* c) { return dim3((unsigned)((c->p.nx / 2 + 127) / 128), c->p.ny, c->p.nz); }
 

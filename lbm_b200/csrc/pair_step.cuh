@@ -347,7 +347,7 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 #define LBM_PAIR_MIN_BLOCKS 5
 #endif
 // Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
-// ihrr = 1, nx even and Q * dstride < 2^31.
+// ihrr = 1 and nx even; offsets are 64-bit, so any state size.
 template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
 __global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
                                                                         StepArgs a) {

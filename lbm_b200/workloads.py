@@ -49,6 +49,8 @@ class Workload:
 SPHERE_128 = Workload("sphere_q27_128x64x64", 128, 64, 64, 27, steps=200, sphere=(32, 32, 32, 8))
 CHANNEL_Q27 = Workload("turb_inflow_q27_512x256x256", 512, 256, 256, 27, steps=1000, lturb=True, ampl=1.0e-4)
 CHANNEL_Q19 = CHANNEL_Q27.with_(name="turb_inflow_q19_512x256x256", nl=19)
+# the channel at 84 M cells: a state buffer of 2.4 G elements (64-bit offsets)
+CHANNEL_Q27_LARGE = CHANNEL_Q27.with_(name="turb_inflow_q27_512x512x320", ny=512, nz=320)
 # one eighth of the channel, for profiler captures that must stay small
 CHANNEL_Q27_SMALL = CHANNEL_Q27.with_(name="turb_inflow_q27_256x128x128", nx=256, ny=128, nz=128)
 CHANNEL_Q19_SMALL = CHANNEL_Q27_SMALL.with_(name="turb_inflow_q19_256x128x128", nl=19)
@@ -104,8 +106,8 @@ def ensemble_members(n: int = 64, seed: int = 0, nl: int = 19, storage_steps: in
     return out
 
 
-WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_SMALL, CHANNEL_Q19_SMALL,
-                                 CITY_Q27, CITY_Q27_REDUCED, ADJOINT_Q19)}
+WORKLOADS = {w.name: w for w in (SPHERE_128, CHANNEL_Q27, CHANNEL_Q19, CHANNEL_Q27_LARGE, CHANNEL_Q27_SMALL,
+                                 CHANNEL_Q19_SMALL, CITY_Q27, CITY_Q27_REDUCED, ADJOINT_Q19)}
 
 
 def initial_macro(wl: Workload, dtype=np.float32):
