@@ -216,7 +216,6 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
             break;
         }
         e->m.push_back(c);
-        if (!c->idx32) rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: grid too large for the ensemble kernels", k);
     }
     const size_t nm = e->m.size();
     if (rc == LBM_OK) rc = echeck(e, cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking), "cudaStreamCreate");

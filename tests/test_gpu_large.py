@@ -38,24 +38,32 @@ def tile_j(a, m, axis=1):
     return out
 
 
-def run(p, state, blank, uvel, turb, steps):
-    from lbm_b200 import Lbm
-    L = Lbm(p)
+def prepare(L, state, blank, uvel, turb):
     if blank is not None:
         L.set_solids(blank)
     L.set_inflow(uvel)
     if turb is not None:
         L.set_turbulence(*turb, nrturb=turb[0].shape[0] - 1, ampl=1.0e-3)
     L.state_import(*state)
-    L.step(steps)
+
+
+def result(L):
     f1, f2 = L.empty_f(), L.empty_f()
     L.state_export(f1, f2)
     m = [L.empty_s() for _ in range(4)]
     L.get_macro(*m)
     torch.cuda.synchronize()
-    status = L.status()
+    return [f1, f2, *m], L.status()
+
+
+def run(p, state, blank, uvel, turb, steps):
+    from lbm_b200 import Lbm
+    L = Lbm(p)
+    prepare(L, state, blank, uvel, turb)
+    L.step(steps)
+    out = result(L)
     L.close()
-    return [f1, f2, *m], status
+    return out
 
 
 def same_bits(big, small, m):
@@ -69,9 +77,12 @@ def same_bits(big, small, m):
     return bool(torch.equal(tiles.view(torch.int32), small[:, 1:-1].unsqueeze(1).expand_as(tiles).view(torch.int32)))
 
 
-@pytest.mark.parametrize("codes,storage,turbulence", [((1, 0, 12), "f32", True), ((1, 0, 12), "f16", True),
-                                                     ((0, 0, 0), "f32", False)])
-def test_state_past_2_to_31_elements(codes, storage, turbulence):
+@pytest.mark.parametrize("codes,storage,turbulence,ensemble", [((1, 0, 12), "f32", True, True),
+                                                              ((1, 0, 12), "f16", True, False),
+                                                              ((0, 0, 0), "f32", False, False)])
+def test_state_past_2_to_31_elements(codes, storage, turbulence, ensemble):
+    """ensemble: the small and the large domain also run as the two members of
+    one batched ensemble, which must reproduce their separate runs bit for bit."""
     ib, jb, kb = codes
     wl = W.Workload("large", 128, NY_SMALL, 62, 27, steps=6, ibnd=ib, jbnd=jb, kbnd=kb, noise=3e-3,
                     sphere=(40, 8, 20, 5))
@@ -91,13 +102,26 @@ def test_state_past_2_to_31_elements(codes, storage, turbulence):
     pitch = ((big_wl.nx + 34 + 31) // 32) * 32
     assert 27 * (big_wl.ny + 2) * (big_wl.nz + 2) * pitch > 2 ** 31
     big_state = [tile_j(a, COPIES) for a in small_state]
-    del small_state
     turb_b = None
     if turbulence:
         turb_b = [t.repeat(1, 1, COPIES) for t in turb_s]
-    big, st_big = run(p_big, big_state, tile_j(blank_s, COPIES), uvel_d, turb_b, wl.steps)
-    del big_state
+    blank_b = tile_j(blank_s, COPIES)
+    big, st_big = run(p_big, big_state, blank_b, uvel_d, turb_b, wl.steps)
     assert st_small == 0 and st_big == 0
     assert torch.isfinite(small[0]).all()
     for name, b, s in zip(("f1", "f2", "rho", "u", "v", "w"), big, small):
         assert same_bits(b, s, COPIES), name
+    if ensemble:
+        from lbm_b200 import Ensemble
+        ens = Ensemble([p_small, p_big])
+        prepare(ens.members[0], small_state, blank_s, uvel_d, turb_s)
+        prepare(ens.members[1], big_state, blank_b, uvel_d, turb_b)
+        del big_state
+        ens.step(wl.steps)
+        for alone, L in ((small, ens.members[0]), (big, ens.members[1])):
+            batched, st = result(L)
+            assert st == 0
+            for name, a, b in zip(("f1", "f2", "rho", "u", "v", "w"), batched, alone):
+                assert torch.equal(a.view(torch.int32), b.view(torch.int32)), "ensemble " + name
+            del batched
+        ens.close()
