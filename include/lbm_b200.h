@@ -127,12 +127,13 @@ int lbm_compute_f(lbm_ctx* ctx, float* f, const float* feq);
 /* boundarycond(f1,f2,uvel,...)     m_boundarycond.F90:14 (tracer/pottemp are off this path) */
 int lbm_boundarycond(lbm_ctx* ctx, float* f1, float* f2, const float* uvel);
 
-/* solids(f,blanking)               m_solids.F90:3; blanking is logical(4) over the ghost-inclusive grid */
 /* call forcings_apply(f1,external_forcing,rho,u,v,w)    m_forcings_apply.F90:3-64
  * external_forcing(3,0:nx+1,0:ny+1,0:nz+1): f += feq2(rho, u - F/rho) - feq2(rho, u) at
  * interior cells with rho > 0 (main.F90:306, between postcoll and solids) */
 int lbm_forcings_apply(lbm_ctx* ctx, float* f, const float* external_forcing, const float* rho, const float* u,
                        const float* v, const float* w);
+
+/* solids(f,blanking)               m_solids.F90:3; blanking is logical(4) over the ghost-inclusive grid */
 int lbm_solids(lbm_ctx* ctx, float* f, const int32_t* blanking);
 
 /* inflow_turbulence_forcing(rho,u,v,w,ampl,it,nrturb)  m_inflow_turbulence_forcing.F90:5.
@@ -147,6 +148,37 @@ int lbm_inflow_turbulence_apply(lbm_ctx* ctx, float* f, const float* df);
 
 /* fillghosts(f)                    m_fillghosts.F90:4 */
 int lbm_fillghosts(lbm_ctx* ctx, float* f);
+
+/* ---- per-call entry points of the DP build ----------------------------------
+ * The reference built with DP=1 (src/makefile:82-86: -DDOUBLE_PRECISION with
+ * -fdefault-real-8 or -r8) holds every real in double precision, tiny() and
+ * eps = sqrt(tiny) included.  Each _f64 entry point takes the same arguments
+ * as the entry point above it with double arrays, runs the same kernel
+ * computing in FP64, and has the same error behaviour.  The context's
+ * kinevisc, smagorinsky, rho0 and udir enter these as doubles converted from
+ * lbm_params; lbm_set_params_f64 gives them at double precision instead
+ * (the DP build reads them from its infile as real(8), m_readinfile.F90:22,129). */
+int lbm_set_params_f64(lbm_ctx* ctx, double kinevisc, double smagorinsky, double rho0, double udir);
+int lbm_fequil3_f64(lbm_ctx* ctx, double* feq, const double* rho, const double* u, const double* v,
+                    const double* w);
+int lbm_postcoll_f64(lbm_ctx* ctx, double* f, double* tau, const double* rho, const double* u, const double* v,
+                     const double* w, const double* ablvisc);
+int lbm_drift_f64(lbm_ctx* ctx, double* f, const double* feq);
+int lbm_macrovars_f64(lbm_ctx* ctx, double* rho, double* u, double* v, double* w, const double* f);
+int lbm_regularization_f64(lbm_ctx* ctx, double* f, const double* feq, const double* u, const double* v,
+                           const double* w);
+int lbm_vreman_f64(lbm_ctx* ctx, const double* f, double* tau);
+int lbm_compute_fneq_f64(lbm_ctx* ctx, double* f, const double* feq);
+int lbm_compute_f_f64(lbm_ctx* ctx, double* f, const double* feq);
+int lbm_boundarycond_f64(lbm_ctx* ctx, double* f1, double* f2, const double* uvel);
+int lbm_forcings_apply_f64(lbm_ctx* ctx, double* f, const double* external_forcing, const double* rho,
+                           const double* u, const double* v, const double* w);
+int lbm_solids_f64(lbm_ctx* ctx, double* f, const int32_t* blanking);
+int lbm_inflow_turbulence_forcing_f64(lbm_ctx* ctx, double* df, const double* rho, const double* u,
+                                      const double* v, const double* w, const double* uu, const double* vv,
+                                      const double* ww, double ampl, int32_t it, int32_t nrturb);
+int lbm_inflow_turbulence_apply_f64(lbm_ctx* ctx, double* f, const double* df);
+int lbm_fillghosts_f64(lbm_ctx* ctx, double* f);
 
 /* ---- fused state API ---------------------------------------------------------
  * The state mirrors main.F90 between time steps: f1 (pre-collision, after

@@ -117,6 +117,74 @@ module lbm_b200_iface
          type(c_ptr), value :: ctx, f
       end function
 
+      ! ---- the DP build (DP=1, every real in double precision): the same calls on
+      ! real(c_double) device arrays, passed as c_devloc / c_loc pointers -------------
+      integer(c_int) function lbm_set_params_f64(ctx, kinevisc, smagorinsky, rho0, udir) &
+            bind(C, name="lbm_set_params_f64")
+         import :: c_ptr, c_int, c_double
+         type(c_ptr), value    :: ctx
+         real(c_double), value :: kinevisc, smagorinsky, rho0, udir
+      end function
+      integer(c_int) function lbm_fequil3_f64(ctx, feq, rho, u, v, w) bind(C, name="lbm_fequil3_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, feq, rho, u, v, w
+      end function
+      integer(c_int) function lbm_postcoll_f64(ctx, f, tau, rho, u, v, w, ablvisc) bind(C, name="lbm_postcoll_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, tau, rho, u, v, w, ablvisc
+      end function
+      integer(c_int) function lbm_drift_f64(ctx, f, feq) bind(C, name="lbm_drift_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      integer(c_int) function lbm_macrovars_f64(ctx, rho, u, v, w, f) bind(C, name="lbm_macrovars_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, rho, u, v, w, f
+      end function
+      integer(c_int) function lbm_regularization_f64(ctx, f, feq, u, v, w) bind(C, name="lbm_regularization_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq, u, v, w
+      end function
+      integer(c_int) function lbm_vreman_f64(ctx, f, tau) bind(C, name="lbm_vreman_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, tau
+      end function
+      integer(c_int) function lbm_compute_fneq_f64(ctx, f, feq) bind(C, name="lbm_compute_fneq_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      integer(c_int) function lbm_compute_f_f64(ctx, f, feq) bind(C, name="lbm_compute_f_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, feq
+      end function
+      integer(c_int) function lbm_boundarycond_f64(ctx, f1, f2, uvel) bind(C, name="lbm_boundarycond_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f1, f2, uvel
+      end function
+      integer(c_int) function lbm_forcings_apply_f64(ctx, f, external_forcing, rho, u, v, w) bind(C, name="lbm_forcings_apply_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, external_forcing, rho, u, v, w
+      end function
+      integer(c_int) function lbm_solids_f64(ctx, f, blanking) bind(C, name="lbm_solids_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, blanking
+      end function
+      integer(c_int) function lbm_inflow_turbulence_forcing_f64(ctx, df, rho, u, v, w, uu, vv, ww, ampl, it, &
+            nrturb) bind(C, name="lbm_inflow_turbulence_forcing_f64")
+         import :: c_ptr, c_int, c_double, c_int32_t
+         type(c_ptr), value        :: ctx, df, rho, u, v, w, uu, vv, ww
+         real(c_double), value     :: ampl
+         integer(c_int32_t), value :: it, nrturb
+      end function
+      integer(c_int) function lbm_inflow_turbulence_apply_f64(ctx, f, df) bind(C, name="lbm_inflow_turbulence_apply_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f, df
+      end function
+      integer(c_int) function lbm_fillghosts_f64(ctx, f) bind(C, name="lbm_fillghosts_f64")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: ctx, f
+      end function
+
       ! ---- fused state API ----------------------------------------------------------------
       integer(c_int) function lbm_state_import(ctx, f1, f2, rho, u, v, w, it) bind(C, name="lbm_state_import")
          import :: c_ptr, c_int, c_int32_t

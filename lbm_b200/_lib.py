@@ -47,6 +47,7 @@ class LbmParams(ctypes.Structure):
 P = ctypes.c_void_p
 I = ctypes.c_int32
 F = ctypes.c_float
+D = ctypes.c_double
 
 # name -> argument types (all return int32 status except lbm_last_error)
 SIGNATURES = {
@@ -68,6 +69,22 @@ SIGNATURES = {
     "lbm_inflow_turbulence_forcing": [P, P, P, P, P, P, P, P, P, F, I, I],
     "lbm_inflow_turbulence_apply": [P, P, P],
     "lbm_fillghosts": [P, P],
+    # the DP build's per-call entry points: the same arguments with double arrays
+    "lbm_set_params_f64": [P, D, D, D, D],
+    "lbm_fequil3_f64": [P, P, P, P, P, P],
+    "lbm_postcoll_f64": [P, P, P, P, P, P, P, P],
+    "lbm_drift_f64": [P, P, P],
+    "lbm_macrovars_f64": [P, P, P, P, P, P],
+    "lbm_regularization_f64": [P, P, P, P, P, P],
+    "lbm_vreman_f64": [P, P, P],
+    "lbm_compute_fneq_f64": [P, P, P],
+    "lbm_compute_f_f64": [P, P, P],
+    "lbm_boundarycond_f64": [P, P, P, P],
+    "lbm_forcings_apply_f64": [P, P, P, P, P, P, P],
+    "lbm_solids_f64": [P, P, P],
+    "lbm_inflow_turbulence_forcing_f64": [P, P, P, P, P, P, P, P, P, D, I, I],
+    "lbm_inflow_turbulence_apply_f64": [P, P, P],
+    "lbm_fillghosts_f64": [P, P],
     "lbm_state_import": [P, P, P, P, P, P, P, I],
     "lbm_state_export": [P, P, P],
     "lbm_get_macro": [P, P, P, P, P],

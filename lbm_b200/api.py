@@ -11,6 +11,9 @@ torch tensors in the reference layout viewed in C order:
 * ``turbulence_df(nl,ny,nz)``     -> ``float32[nz, ny, nl]``
 * ``lblanking`` logical(4)        -> ``int32[nz+2, ny+2, nx+2]``
 
+The per-call methods also take float64 arrays: they then run the ``_f64``
+entry points, the reference's DP build (every real in double precision).
+
 torch is used for device memory and streams only; all arithmetic runs in the
 library's sm_100a kernels.  Errors raise :class:`LbmError`.
 """
@@ -84,6 +87,7 @@ class Lbm:
             self.h = h
         self.stream = stream if stream is not None else torch.cuda.current_stream()
         self._call("lbm_set_stream", ctypes.c_void_p(self.stream.cuda_stream))
+        self.set_params_f64()      # the float64 calls take the Params values at double precision
 
     def close(self):
         if getattr(self, "h", None):
@@ -119,82 +123,112 @@ class Lbm:
             raise LbmError(_lib.LBM_ERR_ARG, "%s must be contiguous %s%s, got %s%s" % (
                 name, dtype, tuple(shape), t.dtype, tuple(t.shape)))
 
-    def _f(self, *ts):
+    def _f(self, *ts, dtype=torch.float32):
         for t in ts:
-            self._chk(t, self.p.fshape, name="f")
+            self._chk(t, self.p.fshape, dtype, name="f")
 
-    def _s(self, *ts):
+    def _s(self, *ts, dtype=torch.float32):
         for t in ts:
-            self._chk(t, self.p.sshape, name="scalar field")
+            self._chk(t, self.p.sshape, dtype, name="scalar field")
+
+    @staticmethod
+    def _real(t):
+        """(entry-point suffix, dtype) of a per-call call from its first array:
+        float32 runs the reference's default build, float64 its DP build
+        (the ``_f64`` entry points); every array of the call has that dtype."""
+        if t is not None and t.dtype == torch.float64:
+            return "_f64", torch.float64
+        return "", torch.float32
 
     # ---- tensors -----------------------------------------------------------------
-    def empty_f(self):
-        return torch.zeros(self.p.fshape, dtype=torch.float32, device="cuda")
+    def empty_f(self, dtype=torch.float32):
+        return torch.zeros(self.p.fshape, dtype=dtype, device="cuda")
 
-    def empty_s(self):
-        return torch.zeros(self.p.sshape, dtype=torch.float32, device="cuda")
+    def empty_s(self, dtype=torch.float32):
+        return torch.zeros(self.p.sshape, dtype=dtype, device="cuda")
 
     # ---- reference subroutines -------------------------------------------------------
+    def set_params_f64(self, kinevisc=None, smagorinsky=None, rho0=None, udir=None):
+        """kinevisc, smagorinsky, rho0 and udir of the float64 calls at double
+        precision (default: the Params values)."""
+        p = self.p
+        self._call("lbm_set_params_f64", ctypes.c_double(p.kinevisc if kinevisc is None else kinevisc),
+                   ctypes.c_double(p.smagorinsky if smagorinsky is None else smagorinsky),
+                   ctypes.c_double(p.rho0 if rho0 is None else rho0), ctypes.c_double(p.udir if udir is None else udir))
+
     def fequil3(self, feq, rho, u, v, w):
-        self._f(feq)
-        self._s(rho, u, v, w)
-        self._call("lbm_fequil3", _ptr(feq), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+        sfx, dt = self._real(feq)
+        self._f(feq, dtype=dt)
+        self._s(rho, u, v, w, dtype=dt)
+        self._call("lbm_fequil3" + sfx, _ptr(feq), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
 
     def postcoll(self, f, tau, rho, u, v, w, ablvisc=None):
-        self._f(f)
-        self._s(tau, rho, u, v, w)
-        self._chk(ablvisc, (self.p.nz,), name="ablvisc")
-        self._call("lbm_postcoll", _ptr(f), _ptr(tau), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(ablvisc))
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
+        self._s(tau, rho, u, v, w, dtype=dt)
+        self._chk(ablvisc, (self.p.nz,), dt, name="ablvisc")
+        self._call("lbm_postcoll" + sfx, _ptr(f), _ptr(tau), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(ablvisc))
 
     def drift(self, f, feq):
-        self._f(f, feq)
-        self._call("lbm_drift", _ptr(f), _ptr(feq))
+        sfx, dt = self._real(f)
+        self._f(f, feq, dtype=dt)
+        self._call("lbm_drift" + sfx, _ptr(f), _ptr(feq))
 
     def macrovars(self, rho, u, v, w, f):
-        self._s(rho, u, v, w)
-        self._f(f)
-        self._call("lbm_macrovars", _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(f))
+        sfx, dt = self._real(f)
+        self._s(rho, u, v, w, dtype=dt)
+        self._f(f, dtype=dt)
+        self._call("lbm_macrovars" + sfx, _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(f))
 
     def regularization(self, f, feq, u, v, w):
-        self._f(f, feq)
-        self._s(u, v, w)
-        self._call("lbm_regularization", _ptr(f), _ptr(feq), _ptr(u), _ptr(v), _ptr(w))
+        sfx, dt = self._real(f)
+        self._f(f, feq, dtype=dt)
+        self._s(u, v, w, dtype=dt)
+        self._call("lbm_regularization" + sfx, _ptr(f), _ptr(feq), _ptr(u), _ptr(v), _ptr(w))
 
     def vreman(self, f, tau):
-        self._f(f)
-        self._s(tau)
-        self._call("lbm_vreman", _ptr(f), _ptr(tau))
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
+        self._s(tau, dtype=dt)
+        self._call("lbm_vreman" + sfx, _ptr(f), _ptr(tau))
 
     def compute_fneq(self, f, feq):
-        self._f(f, feq)
-        self._call("lbm_compute_fneq", _ptr(f), _ptr(feq))
+        sfx, dt = self._real(f)
+        self._f(f, feq, dtype=dt)
+        self._call("lbm_compute_fneq" + sfx, _ptr(f), _ptr(feq))
 
     def compute_f(self, f, feq):
-        self._f(f, feq)
-        self._call("lbm_compute_f", _ptr(f), _ptr(feq))
+        sfx, dt = self._real(f)
+        self._f(f, feq, dtype=dt)
+        self._call("lbm_compute_f" + sfx, _ptr(f), _ptr(feq))
 
     def boundarycond(self, f1, f2, uvel):
-        self._f(f1, f2)
-        self._chk(uvel, (self.p.nz,), name="uvel")
-        self._call("lbm_boundarycond", _ptr(f1), _ptr(f2), _ptr(uvel))
+        sfx, dt = self._real(f1)
+        self._f(f1, f2, dtype=dt)
+        self._chk(uvel, (self.p.nz,), dt, name="uvel")
+        self._call("lbm_boundarycond" + sfx, _ptr(f1), _ptr(f2), _ptr(uvel))
 
     def solids(self, f, blanking):
-        self._f(f)
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
         self._chk(blanking, self.p.sshape, torch.int32, name="blanking")
-        self._call("lbm_solids", _ptr(f), _ptr(blanking))
+        self._call("lbm_solids" + sfx, _ptr(f), _ptr(blanking))
 
     def inflow_turbulence_forcing(self, df, rho, u, v, w, uu, vv, ww, ampl, it, nrturb):
-        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
-        self._s(rho, u, v, w)
+        sfx, dt = self._real(df)
+        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), dt, name="turbulence_df")
+        self._s(rho, u, v, w, dtype=dt)
         for t in (uu, vv, ww):
-            self._chk(t, (nrturb + 1, self.p.nz, self.p.ny), name="uu/vv/ww")
-        self._call("lbm_inflow_turbulence_forcing", _ptr(df), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(uu),
-                   _ptr(vv), _ptr(ww), ctypes.c_float(ampl), ctypes.c_int32(it), ctypes.c_int32(nrturb))
+            self._chk(t, (nrturb + 1, self.p.nz, self.p.ny), dt, name="uu/vv/ww")
+        a = ctypes.c_double(ampl) if sfx else ctypes.c_float(ampl)
+        self._call("lbm_inflow_turbulence_forcing" + sfx, _ptr(df), _ptr(rho), _ptr(u), _ptr(v), _ptr(w), _ptr(uu),
+                   _ptr(vv), _ptr(ww), a, ctypes.c_int32(it), ctypes.c_int32(nrturb))
 
     def inflow_turbulence_apply(self, f, df):
-        self._f(f)
-        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), name="turbulence_df")
-        self._call("lbm_inflow_turbulence_apply", _ptr(f), _ptr(df))
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
+        self._chk(df, (self.p.nz, self.p.ny, self.p.nl), dt, name="turbulence_df")
+        self._call("lbm_inflow_turbulence_apply" + sfx, _ptr(f), _ptr(df))
 
     def inflow_turbulence_compute(self, uu, vv, ww, nrturb, seed, rr=None):
         """Fill uu, vv, ww (and rr) -- float32 (nrturb+1, nz, ny) -- with the inflow-turbulence levels."""
@@ -264,8 +298,9 @@ class Lbm:
         self._call("lbm_state_adjoint_export", _ptr(fhat), _ptr(A))
 
     def fillghosts(self, f):
-        self._f(f)
-        self._call("lbm_fillghosts", _ptr(f))
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
+        self._call("lbm_fillghosts" + sfx, _ptr(f))
 
     # ---- fused state ------------------------------------------------------------------
     def state_import(self, f1, f2, rho, u, v, w, it=0):
@@ -296,11 +331,13 @@ class Lbm:
                    ctypes.c_float(ampl))
 
     def forcings_apply(self, f, external_forcing, rho, u, v, w):
-        """external_forcing: float32 (nz+2, ny+2, nx+2, 3), the reference's external_forcing(3,0:nx+1,...)."""
-        self._f(f)
-        self._chk(external_forcing, self.p.sshape + (3,), name="external_forcing")
-        self._s(rho, u, v, w)
-        self._call("lbm_forcings_apply", _ptr(f), _ptr(external_forcing), _ptr(rho), _ptr(u), _ptr(v), _ptr(w))
+        """external_forcing: (nz+2, ny+2, nx+2, 3), the reference's external_forcing(3,0:nx+1,...)."""
+        sfx, dt = self._real(f)
+        self._f(f, dtype=dt)
+        self._chk(external_forcing, self.p.sshape + (3,), dt, name="external_forcing")
+        self._s(rho, u, v, w, dtype=dt)
+        self._call("lbm_forcings_apply" + sfx, _ptr(f), _ptr(external_forcing), _ptr(rho), _ptr(u), _ptr(v),
+                   _ptr(w))
 
     def set_forcing(self, external_forcing):
         """Fused-step forcing field (read at every step; keep the tensor alive), or None."""

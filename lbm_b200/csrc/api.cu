@@ -7,6 +7,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lbm_b200.h"
@@ -41,6 +42,8 @@ struct lbm_ctx {
     RefGrid rg;
     SoaGrid sg;
     CollideParams cp;
+    CollideParamsT<double> cpd;      // the FP64 entry points' parameters (the reference's DP build)
+    double rho0d = 1.0, cosdd = 1.0, sindd = 0.0;
     FacePairs face[3][2];
     bool face_on[3] = {false, false, false};
     EdgeSet edges[3];
@@ -288,9 +291,27 @@ void setup_boundaries(lbm_ctx* c) {
     c->sind = sinf(c->p.udir * pi / 180.0f);
 }
 
+// Parameters of the FP64 entry points, as the reference's DP build (-r8) holds
+// them: every real in double precision, tiny() and eps = sqrt(tiny) of double
+// (m_postcoll.F90:46-47), pi the same literal as in single precision
+// (m_boundary_i_inflow_kernel.F90:191-193).
+void set_params_f64(lbm_ctx* c, double kinevisc, double smagorinsky, double rho0, double udir) {
+    c->cpd.kinevisc = kinevisc;
+    c->cpd.cvre = 2.5 * smagorinsky * smagorinsky;
+    c->cpd.eps = std::sqrt(lat_tiny<double>());
+    c->cpd.tau0 = 3.0 * kinevisc + 0.5;
+    c->cpd.ibgk = c->p.ibgk;
+    c->cpd.ihrr = c->p.ihrr;
+    c->cpd.ivreman = c->p.ivreman;
+    c->rho0d = rho0;
+    const double pi = 3.1415927410125732;
+    c->cosdd = std::cos(udir * pi / 180.0);
+    c->sindd = std::sin(udir * pi / 180.0);
+}
+
 // boundarycond in the dispatch order of m_boundarycond.F90:14-468
 template <int Q, typename Acc>
-int run_bc(lbm_ctx* c, Acc f1, Acc f2, const float* uvel) {
+int run_bc(lbm_ctx* c, Acc f1, Acc f2, const typename Acc::real* uvel) {
     const int nx = c->p.nx, ny = c->p.ny, nz = c->p.nz, nl = c->p.nl;
     cudaStream_t s = c->stream;
     auto periodic = [&](int axis) {
@@ -324,7 +345,10 @@ int run_bc(lbm_ctx* c, Acc f1, Acc f2, const float* uvel) {
         c->launches++;
     }
     if (c->p.ibnd == 1) {
-        k_inflow<Q, Acc><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(f1, uvel, c->p.rho0, c->cosd, c->sind);
+        if constexpr (std::is_same<typename Acc::real, double>::value)
+            k_inflow<Q, Acc><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(f1, uvel, c->rho0d, c->cosdd, c->sindd);
+        else
+            k_inflow<Q, Acc><<<dim3((ny + 127) / 128, nz), 128, 0, s>>>(f1, uvel, c->p.rho0, c->cosd, c->sind);
         c->launches++;
     }
     for (int a = 0; a < 3; ++a)
@@ -333,9 +357,9 @@ int run_bc(lbm_ctx* c, Acc f1, Acc f2, const float* uvel) {
     return LBM_OK;
 }
 
-template <int Q>
-int bc_ref(lbm_ctx* c, float* f1, float* f2, const float* uvel) {
-    AosAcc a1{f1, c->rg}, a2{f2, c->rg};
+template <int Q, typename R>
+int bc_ref(lbm_ctx* c, R* f1, R* f2, const R* uvel) {
+    AosAccT<R> a1{f1, c->rg}, a2{f2, c->rg};
     return run_bc<Q>(c, a1, a2, uvel);
 }
 
@@ -612,6 +636,151 @@ void launch_sum_pre(lbm_ctx* c) {
         }                                                                              \
     } while (0)
 
+// ---- per-call kernels in either arithmetic type: R = float (the reference's
+// default build) or double (its DP build); the entry points check arguments ----
+template <typename R>
+const CollideParamsT<R>& cp_of(const lbm_ctx* c);
+template <>
+const CollideParamsT<float>& cp_of<float>(const lbm_ctx* c) { return c->cp; }
+template <>
+const CollideParamsT<double>& cp_of<double>(const lbm_ctx* c) { return c->cpd; }
+
+dim3 interior_rows(const lbm_ctx* c) { return dim3((c->p.nx + 127) / 128, c->p.ny, c->p.nz); }
+
+template <typename R>
+int fequil3_run(lbm_ctx* c, R* feq, const R* rho, const R* u, const R* v, const R* w) {
+    if (c->p.nl == 27) k_ref_fequil3<27, R><<<interior_rows(c), 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
+    else k_ref_fequil3<19, R><<<interior_rows(c), 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
+    c->launches++;
+    LBM_LAUNCHED(c, "fequil3");
+    return LBM_OK;
+}
+
+template <typename R>
+int postcoll_run(lbm_ctx* c, R* f, R* tau, const R* rho, const R* u, const R* v, const R* w, const R* ablvisc) {
+    const CollideParamsT<R>& cp = cp_of<R>(c);
+    if (c->p.nl == 27) k_ref_postcoll<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, cp);
+    else k_ref_postcoll<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, cp);
+    c->launches++;
+    LBM_LAUNCHED(c, "postcoll");
+    return LBM_OK;
+}
+
+template <typename R>
+int drift_run(lbm_ctx* c, R* f, const R* feq) {
+    if (f == feq) return fail(c, LBM_ERR_ARG, "drift: f and feq must be distinct buffers");
+    if (c->p.nl == 27) k_ref_drift<27, R><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
+    else k_ref_drift<19, R><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "drift");
+    return LBM_OK;
+}
+
+template <typename R>
+int macrovars_run(lbm_ctx* c, R* rho, R* u, R* v, R* w, const R* f) {
+    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
+    if (c->p.nl == 27) k_ref_macrovars<27, R><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
+    else k_ref_macrovars<19, R><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "macrovars");
+    return LBM_OK;
+}
+
+template <typename R>
+int regularization_run(lbm_ctx* c, R* f, const R* feq, const R* u, const R* v, const R* w) {
+    if (c->p.nl == 27) k_ref_regularization<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
+    else k_ref_regularization<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "regularization");
+    return LBM_OK;
+}
+
+template <typename R>
+int vreman_run(lbm_ctx* c, const R* f, R* tau) {
+    if (c->p.ivreman != 1) return LBM_OK;   // m_vreman.F90:211-213
+    const CollideParamsT<R>& cp = cp_of<R>(c);
+    if (c->p.nl == 27) k_ref_vreman<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, c->rg, cp);
+    else k_ref_vreman<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, c->rg, cp);
+    c->launches++;
+    LBM_LAUNCHED(c, "vreman");
+    return LBM_OK;
+}
+
+// compute_fneq (sgn < 0) / compute_f (sgn > 0)
+template <typename R>
+int axpy_run(lbm_ctx* c, R* f, const R* feq, int sgn, const char* what) {
+    const long long n = c->rg.ncell() * c->p.nl;
+    k_ref_axpy<R><<<148 * 8, 256, 0, c->stream>>>(f, feq, n, sgn);
+    c->launches++;
+    LBM_LAUNCHED(c, what);
+    return LBM_OK;
+}
+
+template <typename R>
+int boundarycond_run(lbm_ctx* c, R* f1, R* f2, const R* uvel) {
+    if (f1 == f2) return fail(c, LBM_ERR_ARG, "boundarycond: f1 and f2 must be distinct buffers");
+    return c->p.nl == 27 ? bc_ref<27, R>(c, f1, f2, uvel) : bc_ref<19, R>(c, f1, f2, uvel);
+}
+
+template <typename R>
+int forcings_apply_run(lbm_ctx* c, R* f, const R* force, const R* rho, const R* u, const R* v, const R* w) {
+    if (c->p.nl == 27) k_ref_forcings_apply<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, force, rho, u, v, w, c->rg);
+    else k_ref_forcings_apply<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, force, rho, u, v, w, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "forcings_apply");
+    return LBM_OK;
+}
+
+template <typename R>
+int solids_run(lbm_ctx* c, R* f, const int32_t* blanking) {
+    if (c->p.nl == 27) k_ref_solids<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, blanking, c->rg);
+    else k_ref_solids<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, blanking, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "solids");
+    return LBM_OK;
+}
+
+template <typename R>
+int turb_forcing_run(lbm_ctx* c, R* df, const R* rho, const R* u, const R* v, const R* w, const R* uu, const R* vv,
+                     const R* ww, R ampl, int32_t it, int32_t nrturb) {
+    if (nrturb <= 0) return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: nrturb must be positive");
+    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
+        return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: iturb_pos outside 1..nx");
+    int lit = it % nrturb;   // m_inflow_turbulence_forcing.F90:45-46
+    if (lit < 0) lit += nrturb;
+    if (lit == 0) lit = nrturb;
+    dim3 grd((c->p.ny + 127) / 128, c->p.nz);
+    if (c->p.nl == 27)
+        k_ref_turb_forcing<27, R><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
+                                                              c->p.ibgk, c->rg);
+    else
+        k_ref_turb_forcing<19, R><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
+                                                              c->p.ibgk, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "inflow_turbulence_forcing");
+    return LBM_OK;
+}
+
+template <typename R>
+int turb_apply_run(lbm_ctx* c, R* f, const R* df) {
+    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
+        return fail(c, LBM_ERR_ARG, "inflow_turbulence_apply: iturb_pos outside 1..nx");
+    dim3 grd((c->p.nl * c->p.ny + 255) / 256, c->p.nz);
+    k_ref_turb_apply<R><<<grd, 256, 0, c->stream>>>(f, df, c->p.iturb_pos, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "inflow_turbulence_apply");
+    return LBM_OK;
+}
+
+template <typename R>
+int fillghosts_run(lbm_ctx* c, R* f) {
+    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
+    k_ref_fillghosts<R><<<grd, 128, 0, c->stream>>>(f, c->rg);
+    c->launches++;
+    LBM_LAUNCHED(c, "fillghosts");
+    return LBM_OK;
+}
+
 }  // namespace
 
 // =============================================================================
@@ -642,6 +811,7 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     c->cp.ibgk = p->ibgk;
     c->cp.ihrr = p->ihrr;
     c->cp.ivreman = p->ivreman;
+    set_params_f64(c, p->kinevisc, p->smagorinsky, p->rho0, p->udir);
     c->elem = (p->storage == LBM_STORE_F16) ? 2 : 4;
     c->idx32 = (long long)p->nl * c->sg.dstride < (1LL << 31);
     setup_boundaries(c);
@@ -717,111 +887,123 @@ int lbm_synchronize(lbm_ctx* c) {
     return cuda_check(c, cudaStreamSynchronize(c->stream), "synchronize");
 }
 
-// ---- per-call entry points ---------------------------------------------------
+// ---- per-call entry points (FP32; the _f64 forms take the DP build's arrays) ----
+// Each pair checks its pointers and runs the same kernels in its own type.
 
 int lbm_fequil3(lbm_ctx* c, float* feq, const float* rho, const float* u, const float* v, const float* w) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, feq); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_fequil3<27><<<grd, 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
-    else k_ref_fequil3<19><<<grd, 128, 0, c->stream>>>(feq, rho, u, v, w, c->rg, c->p.ibgk);
-    c->launches++;
-    LBM_LAUNCHED(c, "fequil3");
-    return LBM_OK;
+    return fequil3_run(c, feq, rho, u, v, w);
+}
+int lbm_fequil3_f64(lbm_ctx* c, double* feq, const double* rho, const double* u, const double* v, const double* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, feq); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    return fequil3_run(c, feq, rho, u, v, w);
 }
 
 int lbm_postcoll(lbm_ctx* c, float* f, float* tau, const float* rho, const float* u, const float* v, const float* w,
                  const float* ablvisc) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, tau); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_postcoll<27><<<grd, 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, c->cp);
-    else k_ref_postcoll<19><<<grd, 128, 0, c->stream>>>(f, tau, rho, u, v, w, ablvisc, c->rg, c->cp);
-    c->launches++;
-    LBM_LAUNCHED(c, "postcoll");
-    return LBM_OK;
+    return postcoll_run(c, f, tau, rho, u, v, w, ablvisc);
+}
+int lbm_postcoll_f64(lbm_ctx* c, double* f, double* tau, const double* rho, const double* u, const double* v,
+                     const double* w, const double* ablvisc) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, tau); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    return postcoll_run(c, f, tau, rho, u, v, w, ablvisc);
 }
 
 int lbm_drift(lbm_ctx* c, float* f, const float* feq) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, feq);
-    if (f == feq) return fail(c, LBM_ERR_ARG, "drift: f and feq must be distinct buffers");
-    if (c->p.nl == 27) k_ref_drift<27><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
-    else k_ref_drift<19><<<dim3(c->p.ny, c->p.nz), 256, 0, c->stream>>>(f, feq, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "drift");
-    return LBM_OK;
+    return drift_run(c, f, feq);
+}
+int lbm_drift_f64(lbm_ctx* c, double* f, const double* feq) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq);
+    return drift_run(c, f, feq);
 }
 
 int lbm_macrovars(lbm_ctx* c, float* rho, float* u, float* v, float* w, const float* f) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, f);
-    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
-    if (c->p.nl == 27) k_ref_macrovars<27><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
-    else k_ref_macrovars<19><<<grd, 128, 0, c->stream>>>(rho, u, v, w, f, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "macrovars");
-    return LBM_OK;
+    return macrovars_run(c, rho, u, v, w, f);
+}
+int lbm_macrovars_f64(lbm_ctx* c, double* rho, double* u, double* v, double* w, const double* f) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, f);
+    return macrovars_run(c, rho, u, v, w, f);
 }
 
 int lbm_regularization(lbm_ctx* c, float* f, const float* feq, const float* u, const float* v, const float* w) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, feq); NEED(c, u); NEED(c, v); NEED(c, w);
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_regularization<27><<<grd, 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
-    else k_ref_regularization<19><<<grd, 128, 0, c->stream>>>(f, feq, u, v, w, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "regularization");
-    return LBM_OK;
+    return regularization_run(c, f, feq, u, v, w);
+}
+int lbm_regularization_f64(lbm_ctx* c, double* f, const double* feq, const double* u, const double* v,
+                           const double* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq); NEED(c, u); NEED(c, v); NEED(c, w);
+    return regularization_run(c, f, feq, u, v, w);
 }
 
 int lbm_vreman(lbm_ctx* c, const float* f, float* tau) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, tau);
-    if (c->p.ivreman != 1) return LBM_OK;   // m_vreman.F90:211-213
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_vreman<27><<<grd, 128, 0, c->stream>>>(f, tau, c->rg, c->cp);
-    else k_ref_vreman<19><<<grd, 128, 0, c->stream>>>(f, tau, c->rg, c->cp);
-    c->launches++;
-    LBM_LAUNCHED(c, "vreman");
-    return LBM_OK;
+    return vreman_run(c, f, tau);
+}
+int lbm_vreman_f64(lbm_ctx* c, const double* f, double* tau) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, tau);
+    return vreman_run(c, f, tau);
 }
 
-static int axpy(lbm_ctx* c, float* f, const float* feq, float sgn, const char* what) {
-    NEED(c, f); NEED(c, feq);
-    const long long n = c->rg.ncell() * c->p.nl;
-    k_ref_axpy<<<148 * 8, 256, 0, c->stream>>>(f, feq, n, sgn);
-    c->launches++;
-    LBM_LAUNCHED(c, what);
-    return LBM_OK;
-}
 int lbm_compute_fneq(lbm_ctx* c, float* f, const float* feq) {
     if (!c) return LBM_ERR_ARG;
-    return axpy(c, f, feq, -1.f, "compute_fneq");
+    NEED(c, f); NEED(c, feq);
+    return axpy_run(c, f, feq, -1, "compute_fneq");
+}
+int lbm_compute_fneq_f64(lbm_ctx* c, double* f, const double* feq) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq);
+    return axpy_run(c, f, feq, -1, "compute_fneq");
 }
 int lbm_compute_f(lbm_ctx* c, float* f, const float* feq) {
     if (!c) return LBM_ERR_ARG;
-    return axpy(c, f, feq, 1.f, "compute_f");
+    NEED(c, f); NEED(c, feq);
+    return axpy_run(c, f, feq, 1, "compute_f");
+}
+int lbm_compute_f_f64(lbm_ctx* c, double* f, const double* feq) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, feq);
+    return axpy_run(c, f, feq, 1, "compute_f");
 }
 
 int lbm_boundarycond(lbm_ctx* c, float* f1, float* f2, const float* uvel) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f1); NEED(c, f2);
     if (c->p.ibnd == 1) NEED(c, uvel);
-    if (f1 == f2) return fail(c, LBM_ERR_ARG, "boundarycond: f1 and f2 must be distinct buffers");
-    return c->p.nl == 27 ? bc_ref<27>(c, f1, f2, uvel) : bc_ref<19>(c, f1, f2, uvel);
+    return boundarycond_run(c, f1, f2, uvel);
+}
+int lbm_boundarycond_f64(lbm_ctx* c, double* f1, double* f2, const double* uvel) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f1); NEED(c, f2);
+    if (c->p.ibnd == 1) NEED(c, uvel);
+    return boundarycond_run(c, f1, f2, uvel);
 }
 
 int lbm_forcings_apply(lbm_ctx* c, float* f, const float* external_forcing, const float* rho, const float* u,
                        const float* v, const float* w) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, external_forcing); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_forcings_apply<27><<<grd, 128, 0, c->stream>>>(f, external_forcing, rho, u, v, w, c->rg);
-    else k_ref_forcings_apply<19><<<grd, 128, 0, c->stream>>>(f, external_forcing, rho, u, v, w, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "forcings_apply");
-    return LBM_OK;
+    return forcings_apply_run(c, f, external_forcing, rho, u, v, w);
+}
+int lbm_forcings_apply_f64(lbm_ctx* c, double* f, const double* external_forcing, const double* rho,
+                           const double* u, const double* v, const double* w) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, external_forcing); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w);
+    return forcings_apply_run(c, f, external_forcing, rho, u, v, w);
 }
 
 int lbm_set_forcing(lbm_ctx* c, const float* external_forcing) {
@@ -833,12 +1015,12 @@ int lbm_set_forcing(lbm_ctx* c, const float* external_forcing) {
 int lbm_solids(lbm_ctx* c, float* f, const int32_t* blanking) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, blanking);
-    dim3 grd((c->p.nx + 127) / 128, c->p.ny, c->p.nz);
-    if (c->p.nl == 27) k_ref_solids<27><<<grd, 128, 0, c->stream>>>(f, blanking, c->rg);
-    else k_ref_solids<19><<<grd, 128, 0, c->stream>>>(f, blanking, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "solids");
-    return LBM_OK;
+    return solids_run(c, f, blanking);
+}
+int lbm_solids_f64(lbm_ctx* c, double* f, const int32_t* blanking) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, blanking);
+    return solids_run(c, f, blanking);
 }
 
 int lbm_inflow_turbulence_forcing(lbm_ctx* c, float* df, const float* rho, const float* u, const float* v,
@@ -846,43 +1028,41 @@ int lbm_inflow_turbulence_forcing(lbm_ctx* c, float* df, const float* rho, const
                                   int32_t it, int32_t nrturb) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, df); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, uu); NEED(c, vv); NEED(c, ww);
-    if (nrturb <= 0) return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: nrturb must be positive");
-    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
-        return fail(c, LBM_ERR_ARG, "inflow_turbulence_forcing: iturb_pos outside 1..nx");
-    int lit = it % nrturb;   // m_inflow_turbulence_forcing.F90:45-46
-    if (lit < 0) lit += nrturb;
-    if (lit == 0) lit = nrturb;
-    dim3 grd((c->p.ny + 127) / 128, c->p.nz);
-    if (c->p.nl == 27)
-        k_ref_turb_forcing<27><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
-                                                           c->p.ibgk, c->rg);
-    else
-        k_ref_turb_forcing<19><<<grd, 128, 0, c->stream>>>(df, rho, u, v, w, uu, vv, ww, ampl, lit, c->p.iturb_pos,
-                                                           c->p.ibgk, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "inflow_turbulence_forcing");
-    return LBM_OK;
+    return turb_forcing_run(c, df, rho, u, v, w, uu, vv, ww, ampl, it, nrturb);
+}
+int lbm_inflow_turbulence_forcing_f64(lbm_ctx* c, double* df, const double* rho, const double* u, const double* v,
+                                      const double* w, const double* uu, const double* vv, const double* ww,
+                                      double ampl, int32_t it, int32_t nrturb) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, df); NEED(c, rho); NEED(c, u); NEED(c, v); NEED(c, w); NEED(c, uu); NEED(c, vv); NEED(c, ww);
+    return turb_forcing_run(c, df, rho, u, v, w, uu, vv, ww, ampl, it, nrturb);
 }
 
 int lbm_inflow_turbulence_apply(lbm_ctx* c, float* f, const float* df) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f); NEED(c, df);
-    if (c->p.iturb_pos < 1 || c->p.iturb_pos > c->p.nx)
-        return fail(c, LBM_ERR_ARG, "inflow_turbulence_apply: iturb_pos outside 1..nx");
-    dim3 grd((c->p.nl * c->p.ny + 255) / 256, c->p.nz);
-    k_ref_turb_apply<<<grd, 256, 0, c->stream>>>(f, df, c->p.iturb_pos, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "inflow_turbulence_apply");
-    return LBM_OK;
+    return turb_apply_run(c, f, df);
+}
+int lbm_inflow_turbulence_apply_f64(lbm_ctx* c, double* f, const double* df) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f); NEED(c, df);
+    return turb_apply_run(c, f, df);
 }
 
 int lbm_fillghosts(lbm_ctx* c, float* f) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, f);
-    dim3 grd((c->p.nx + 2 + 127) / 128, c->p.ny + 2, c->p.nz + 2);
-    k_ref_fillghosts<<<grd, 128, 0, c->stream>>>(f, c->rg);
-    c->launches++;
-    LBM_LAUNCHED(c, "fillghosts");
+    return fillghosts_run(c, f);
+}
+int lbm_fillghosts_f64(lbm_ctx* c, double* f) {
+    if (!c) return LBM_ERR_ARG;
+    NEED(c, f);
+    return fillghosts_run(c, f);
+}
+
+int lbm_set_params_f64(lbm_ctx* c, double kinevisc, double smagorinsky, double rho0, double udir) {
+    if (!c) return LBM_ERR_ARG;
+    set_params_f64(c, kinevisc, smagorinsky, rho0, udir);
     return LBM_OK;
 }
 

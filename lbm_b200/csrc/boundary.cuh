@@ -12,23 +12,28 @@
 
 namespace lbm {
 
-// Accessor for the reference layout f(nl,0:nx+1,0:ny+1,0:nz+1), FP32 absolute values.
-struct AosAcc {
-    float* f;
+// Accessor for the reference layout f(nl,0:nx+1,0:ny+1,0:nz+1), absolute values
+// in the arithmetic type R (FP32, or FP64 for the DP build's entry points).
+template <typename R>
+struct AosAccT {
+    using real = R;
+    R* f;
     RefGrid g;
-    __device__ __forceinline__ float* p(int l, int i, int j, int k) const { return f + g.cell(i, j, k) * g.nl + l; }
-    __device__ __forceinline__ float ld(int l, int i, int j, int k) const { return *p(l, i, j, k); }
-    __device__ __forceinline__ void st(int l, int i, int j, int k, float v) const { *p(l, i, j, k) = v; }
+    __device__ __forceinline__ R* p(int l, int i, int j, int k) const { return f + g.cell(i, j, k) * g.nl + l; }
+    __device__ __forceinline__ R ld(int l, int i, int j, int k) const { return *p(l, i, j, k); }
+    __device__ __forceinline__ void st(int l, int i, int j, int k, R v) const { *p(l, i, j, k) = v; }
     // this(ld,i,j,k) = s(ls,si,sj,sk)
-    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const AosAcc& s, int ls, int si, int sj,
+    __device__ __forceinline__ void cp(int ld, int i, int j, int k, const AosAccT& s, int ls, int si, int sj,
                                        int sk) const {
         *p(ld, i, j, k) = *s.p(ls, si, sj, sk);
     }
 };
+using AosAcc = AosAccT<float>;
 
 // Accessor for the fused state: offsets f - w_l in storage type S.
 template <typename S>
 struct SoaAcc {
+    using real = float;
     S* f;
     SoaGrid g;
     __device__ __forceinline__ S* p(int l, int i, int j, int k) const { return f + (long long)l * g.dstride + g.off(i, j, k); }
@@ -150,24 +155,28 @@ __global__ void k_corners(Acc f1, Acc f2, CornerSet cs) {
 // fghost(l) = f(l,1,j,k) - 2 w_l rho0 (cx u cos + cy u sin) / cs2; directions with
 // cx > 0 take fghost of their opposite.  In offset storage w_l cancels, and
 // opposite directions share w_l, so the same update holds for f - w_l.
+// Acc::real is the arithmetic type (FP32 for the fused state and the default
+// entry point, FP64 for the DP one).
 template <int Q, typename Acc>
-__global__ void k_inflow(Acc f, const float* __restrict__ uvel, float rho0, float cosd, float sind) {
+__global__ void k_inflow(Acc f, const typename Acc::real* __restrict__ uvel, typename Acc::real rho0,
+                         typename Acc::real cosd, typename Acc::real sind) {
+    using R = typename Acc::real;
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int k = blockIdx.y + 1;
     const int nx = f.g.nx;
     if (j > f.g.ny) return;
-    const float uu = uvel[k - 1];
-    const float cs2 = 1.0f / 3.0f;
-    float fg[Q];
+    const R uu = uvel[k - 1];
+    const R cs2 = R(1) / R(3);
+    R fg[Q];
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-        const float wl = lat_w<Q>(l);
-        const float cxl = (float)lat_cx(l), cyl = (float)lat_cy(l);
-        fg[l] = f.ld(l, 1, j, k) - 2.0f * wl * rho0 * (cxl * uu * cosd + cyl * uu * sind) / cs2;
+        const R wl = lat_w<Q, R>(l);
+        const R cxl = (R)lat_cx(l), cyl = (R)lat_cy(l);
+        fg[l] = f.ld(l, 1, j, k) - R(2) * wl * rho0 * (cxl * uu * cosd + cyl * uu * sind) / cs2;
     }
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-        const float v = (lat_cx(l) <= 0) ? fg[l] : fg[lat_opposite(l)];
+        const R v = (lat_cx(l) <= 0) ? fg[l] : fg[lat_opposite(l)];
         f.st(l, 0, j, k, v);
     }
 #pragma unroll

@@ -17,34 +17,43 @@
 // share the even part E and flip the odd part O, so each opposite pair costs
 // one evaluation: f'(+c) = E + O, f'(-c) = E - O.  The solid swap of
 // m_solids.F90:28-32 exchanges exactly these pairs, i.e. negates O.  All
-// arithmetic is FP32 on offsets f' = f - w_l.
+// arithmetic is on offsets f' = f - w_l in the type R: FP32 (the reference's
+// default build) or FP64 (its DP build, where -r8 promotes every real).
 #pragma once
 
 #include "common.cuh"
 
 namespace lbm {
 
-struct CollideParams {
-    float kinevisc;   // nu
-    float cvre;       // 2.5 * smagorinsky^2   (m_postcoll.F90:46)
-    float eps;        // sqrt(tiny(1.0))       (m_postcoll.F90:47)
-    float tau0;       // 3 nu + 0.5, the relaxation time without Vreman (main.F90:262)
+template <typename R>
+struct CollideParamsT {
+    R kinevisc;       // nu
+    R cvre;           // 2.5 * smagorinsky^2   (m_postcoll.F90:46)
+    R eps;            // sqrt(tiny(1.0))       (m_postcoll.F90:47)
+    R tau0;           // 3 nu + 0.5, the relaxation time without Vreman (main.F90:262)
     int ibgk, ihrr, ivreman;
 };
+using CollideParams = CollideParamsT<float>;
 
 // acc += coef * x for coef in {-1, 0, 1} known at compile time after unrolling
 __device__ __forceinline__ void macc(float& acc, int coef, float x) {
     if (coef > 0) acc += x;
     else if (coef < 0) acc -= x;
 }
+__device__ __forceinline__ void macc(double& acc, int coef, double x) {
+    if (coef > 0) acc += x;
+    else if (coef < 0) acc -= x;
+}
 
-struct Moments {
-    float s0, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
+template <typename R>
+struct MomentsT {
+    R s0, jx, jy, jz, pxx, pyy, pzz, pxy, pxz, pyz;
 };
+using Moments = MomentsT<float>;
 
-template <int Q>
-__device__ __forceinline__ Moments moments(const float (&fp)[Q]) {
-    Moments m = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+template <int Q, typename R>
+__device__ __forceinline__ MomentsT<R> moments(const R (&fp)[Q]) {
+    MomentsT<R> m = {R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
@@ -62,8 +71,9 @@ __device__ __forceinline__ Moments moments(const float (&fp)[Q]) {
     return m;
 }
 
-__device__ __forceinline__ float cdot(int cx, int cy, int cz, float x, float y, float z) {
-    float r = 0.f;
+template <typename R>
+__device__ __forceinline__ R cdot(int cx, int cy, int cz, R x, R y, R z) {
+    R r = R(0);
     macc(r, cx, x);
     macc(r, cy, y);
     macc(r, cz, z);
@@ -71,10 +81,12 @@ __device__ __forceinline__ float cdot(int cx, int cy, int cz, float x, float y, 
 }
 
 // Turbulence increment du = ampl * (uu, vv, ww) at the forcing slice.
-struct TurbIn {
+template <typename R>
+struct TurbInT {
     bool on;
-    float dux, duy, duz;
+    R dux, duy, duz;
 };
+using TurbIn = TurbInT<float>;
 
 // Collide one cell in place.  fp holds offsets f' = f - w_l on entry and the
 // post-collision offsets (plus turbulence increment, solid swap) on exit.
@@ -82,84 +94,83 @@ struct TurbIn {
 //   s0, pi: sum f' and the raw second moments of the cell's own f'
 //   tau_in: relaxation time used when ivreman == 0
 // Returns the relaxation time tau of the cell.
-template <int Q>
-__device__ __forceinline__ float collide(float (&fp)[Q], const Moments& m, float drho, float rho, float ux, float uy,
-                                         float uz, const CollideParams& cp, float abl, float tau_in, bool solid,
-                                         const TurbIn& tb) {
-    const float third = 1.0f / 3.0f;
-    const float rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
-    const float axx = m.pxx - m.s0 * third - rux * ux;
-    const float ayy = m.pyy - m.s0 * third - ruy * uy;
-    const float azz = m.pzz - m.s0 * third - ruz * uz;
-    const float axy = m.pxy - rux * uy;
-    const float axz = m.pxz - rux * uz;
-    const float ayz = m.pyz - ruy * uz;
-    const float tr = axx + ayy + azz;
+template <int Q, typename R>
+__device__ __forceinline__ R collide(R (&fp)[Q], const MomentsT<R>& m, R drho, R rho, R ux, R uy, R uz,
+                                     const CollideParamsT<R>& cp, R abl, R tau_in, bool solid, const TurbInT<R>& tb) {
+    const R third = R(1.0) / R(3.0);
+    const R rux = rho * ux, ruy = rho * uy, ruz = rho * uz;
+    const R axx = m.pxx - m.s0 * third - rux * ux;
+    const R ayy = m.pyy - m.s0 * third - ruy * uy;
+    const R azz = m.pzz - m.s0 * third - ruz * uz;
+    const R axy = m.pxy - rux * uy;
+    const R axz = m.pxz - rux * uz;
+    const R ayz = m.pyz - ruy * uz;
+    const R tr = axx + ayy + azz;
 
-    float tau = tau_in;
+    R tau = tau_in;
     if (cp.ivreman) {
         // Vreman (2004) with alpha = a2 (see header); guards as m_postcoll_kernel.F90:270-299
-        float amag = axx * axx + ayy * ayy + azz * azz + 2.0f * (axy * axy + axz * axz + ayz * ayz);
-        amag = fmaxf(amag, 1.17549435e-38f);
-        const float b11 = cp.eps + axx * axx + axy * axy + axz * axz;
-        const float b22 = cp.eps + axy * axy + ayy * ayy + ayz * ayz;
-        const float b33 = cp.eps + axz * axz + ayz * ayz + azz * azz;
-        const float b12 = cp.eps + axx * axy + axy * ayy + axz * ayz;
-        const float b13 = cp.eps + axx * axz + axy * ayz + axz * azz;
-        const float b23 = cp.eps + axy * axz + ayy * ayz + ayz * azz;
-        const float bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
-        const float t = bb / amag;
-        const float nut = (t > cp.eps) ? cp.cvre * sqrtf(t) : 0.0f;
-        tau = 3.0f * (cp.kinevisc + nut + abl) + 0.5f;
+        R amag = axx * axx + ayy * ayy + azz * azz + R(2.0) * (axy * axy + axz * axz + ayz * ayz);
+        amag = real_max(amag, lat_tiny<R>());
+        const R b11 = cp.eps + axx * axx + axy * axy + axz * axz;
+        const R b22 = cp.eps + axy * axy + ayy * ayy + ayz * ayz;
+        const R b33 = cp.eps + axz * axz + ayz * ayz + azz * azz;
+        const R b12 = cp.eps + axx * axy + axy * ayy + axz * ayz;
+        const R b13 = cp.eps + axx * axz + axy * ayz + axz * azz;
+        const R b23 = cp.eps + axy * axz + ayy * ayz + ayz * azz;
+        const R bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+        const R t = bb / amag;
+        const R nut = (t > cp.eps) ? cp.cvre * real_sqrt(t) : R(0.0);
+        tau = R(3.0) * (cp.kinevisc + nut + abl) + R(0.5);
     }
-    const float K = 1.0f - 1.0f / tau;
+    const R K = R(1.0) - R(1.0) / tau;
     const bool cubic = (cp.ibgk == 3);
-    const float usq = ux * ux + uy * uy + uz * uz;
-    const float R45 = 4.5f * rho;
-    const float R45o = cubic ? R45 : 0.0f;
-    const float A0 = drho - 1.5f * rho * usq;              // even equilibrium part / w (cu = 0)
-    const float B0 = 3.0f * rho - (cubic ? R45 * usq : 0.0f);  // odd equilibrium part / (w cu), cu^2 term aside
+    const R usq = ux * ux + uy * uy + uz * uz;
+    const R R45 = R(4.5) * rho;
+    const R R45o = cubic ? R45 : R(0.0);
+    const R A0 = drho - R(1.5) * rho * usq;              // even equilibrium part / w (cu = 0)
+    const R B0 = R(3.0) * rho - (cubic ? R45 * usq : R(0.0));  // odd equilibrium part / (w cu), cu^2 term aside
 
     // turbulence increment feq(rho, u + du) - feq(rho, u) (m_inflow_turbulence_forcing.F90:77-126)
-    float dusq = 0.f;
-    if (tb.on) dusq = tb.dux * (2.0f * ux + tb.dux) + tb.duy * (2.0f * uy + tb.duy) + tb.duz * (2.0f * uz + tb.duz);
-    const float usq2 = usq + dusq;
+    R dusq = R(0);
+    if (tb.on) dusq = tb.dux * (R(2.0) * ux + tb.dux) + tb.duy * (R(2.0) * uy + tb.duy) + tb.duz * (R(2.0) * uz + tb.duz);
+    const R usq2 = usq + dusq;
 
     if (cp.ihrr) {
-        const float C0 = A0 - 1.5f * K * tr;
-        const float D0 = B0 - 4.5f * K * tr;
-        const float K45 = 4.5f * K, K135 = 13.5f * K, K9 = 9.0f * K;
-        const float bxy = 2.0f * axy, bxz = 2.0f * axz, byz = 2.0f * ayz;
-        const float vx = axx * ux + axy * uy + axz * uz;
-        const float vy = axy * ux + ayy * uy + ayz * uz;
-        const float vz = axz * ux + ayz * uy + azz * uz;
+        const R C0 = A0 - R(1.5) * K * tr;
+        const R D0 = B0 - R(4.5) * K * tr;
+        const R K45 = R(4.5) * K, K135 = R(13.5) * K, K9 = R(9.0) * K;
+        const R bxy = R(2.0) * axy, bxz = R(2.0) * axz, byz = R(2.0) * ayz;
+        const R vx = axx * ux + axy * uy + axz * uz;
+        const R vy = axy * ux + ayy * uy + ayz * uz;
+        const R vz = axz * ux + ayz * uy + azz * uz;
         {
-            float e = lat_w<Q>(0) * C0;
-            if (tb.on) e += lat_w<Q>(0) * rho * (-1.5f * dusq);
+            R e = lat_w<Q, R>(0) * C0;
+            if (tb.on) e += lat_w<Q, R>(0) * rho * (-R(1.5) * dusq);
             fp[0] = e;
         }
 #pragma unroll
         for (int l = 1; l < Q; l += 2) {
             const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-            const float w = lat_w<Q>(l);
-            const float cu = cdot(cx, cy, cz, ux, uy, uz);
-            float cac = 0.f;
+            const R w = lat_w<Q, R>(l);
+            const R cu = cdot(cx, cy, cz, ux, uy, uz);
+            R cac = R(0);
             macc(cac, cx * cx, axx);
             macc(cac, cy * cy, ayy);
             macc(cac, cz * cz, azz);
             macc(cac, cx * cy, bxy);
             macc(cac, cx * cz, bxz);
             macc(cac, cy * cz, byz);
-            const float cau = cdot(cx, cy, cz, vx, vy, vz);
-            const float cu2 = cu * cu;
-            float E = w * (C0 + R45 * cu2 + K45 * cac);
-            float O = w * (cu * (D0 + R45o * cu2 + K135 * cac) - K9 * cau);
+            const R cau = cdot(cx, cy, cz, vx, vy, vz);
+            const R cu2 = cu * cu;
+            R E = w * (C0 + R45 * cu2 + K45 * cac);
+            R O = w * (cu * (D0 + R45o * cu2 + K135 * cac) - K9 * cau);
             if (tb.on) {
-                const float dcu = cdot(cx, cy, cz, tb.dux, tb.duy, tb.duz);
-                const float cun = cu + dcu;
-                E += w * rho * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
-                float od = 3.0f * dcu;
-                if (cubic) od += 4.5f * dcu * (cun * cun + cun * cu + cu2 - usq2) - 4.5f * cu * dusq;
+                const R dcu = cdot(cx, cy, cz, tb.dux, tb.duy, tb.duz);
+                const R cun = cu + dcu;
+                E += w * rho * (R(4.5) * dcu * (R(2.0) * cu + dcu) - R(1.5) * dusq);
+                R od = R(3.0) * dcu;
+                if (cubic) od += R(4.5) * dcu * (cun * cun + cun * cu + cu2 - usq2) - R(4.5) * cu * dusq;
                 O += w * rho * od;
             }
             if (solid) O = -O;
@@ -168,29 +179,29 @@ __device__ __forceinline__ float collide(float (&fp)[Q], const Moments& m, float
         }
     } else {
         // plain BGK on the unregularized fneq: f' = (1-K) feq' + K f'
-        const float omk = 1.0f - K;
+        const R omk = R(1.0) - K;
         {
-            float e = omk * lat_w<Q>(0) * A0 + K * fp[0];
-            if (tb.on) e += lat_w<Q>(0) * rho * (-1.5f * dusq);
+            R e = omk * lat_w<Q, R>(0) * A0 + K * fp[0];
+            if (tb.on) e += lat_w<Q, R>(0) * rho * (-R(1.5) * dusq);
             fp[0] = e;
         }
 #pragma unroll
         for (int l = 1; l < Q; l += 2) {
             const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-            const float w = lat_w<Q>(l);
-            const float cu = cdot(cx, cy, cz, ux, uy, uz);
-            const float cu2 = cu * cu;
-            const float Eeq = w * (A0 + R45 * cu2);
-            const float Oeq = w * cu * (B0 + R45o * cu2);
-            float p = omk * (Eeq + Oeq) + K * fp[l];
-            float q = omk * (Eeq - Oeq) + K * fp[l + 1];
+            const R w = lat_w<Q, R>(l);
+            const R cu = cdot(cx, cy, cz, ux, uy, uz);
+            const R cu2 = cu * cu;
+            const R Eeq = w * (A0 + R45 * cu2);
+            const R Oeq = w * cu * (B0 + R45o * cu2);
+            R p = omk * (Eeq + Oeq) + K * fp[l];
+            R q = omk * (Eeq - Oeq) + K * fp[l + 1];
             if (tb.on) {
-                const float dcu = cdot(cx, cy, cz, tb.dux, tb.duy, tb.duz);
-                const float cun = cu + dcu;
-                const float dE = w * rho * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
-                float od = 3.0f * dcu;
-                if (cubic) od += 4.5f * dcu * (cun * cun + cun * cu + cu2 - usq2) - 4.5f * cu * dusq;
-                const float dO = w * rho * od;
+                const R dcu = cdot(cx, cy, cz, tb.dux, tb.duy, tb.duz);
+                const R cun = cu + dcu;
+                const R dE = w * rho * (R(4.5) * dcu * (R(2.0) * cu + dcu) - R(1.5) * dusq);
+                R od = R(3.0) * dcu;
+                if (cubic) od += R(4.5) * dcu * (cun * cun + cun * cu + cu2 - usq2) - R(4.5) * cu * dusq;
+                const R dO = w * rho * od;
                 p += dE + dO;
                 q += dE - dO;
             }

@@ -29,15 +29,28 @@ __host__ __device__ constexpr int lat_cz(int l) {
 __host__ __device__ constexpr int lat_speed2(int l) {
     return lat_cx(l) * lat_cx(l) + lat_cy(l) * lat_cy(l) + lat_cz(l) * lat_cz(l);
 }
-// weights: D3Q19 {1/3, 1/18, 1/36}; D3Q27 {8/27, 2/27, 1/54, 1/216}
-template <int Q>
-__host__ __device__ constexpr float lat_w(int l) {
-    return Q == 19 ? (lat_speed2(l) == 0 ? 1.0f / 3.0f : lat_speed2(l) == 1 ? 1.0f / 18.0f : 1.0f / 36.0f)
-                   : (lat_speed2(l) == 0 ? 8.0f / 27.0f
-                      : lat_speed2(l) == 1 ? 2.0f / 27.0f
-                      : lat_speed2(l) == 2 ? 1.0f / 54.0f
-                                           : 1.0f / 216.0f);
+// weights: D3Q19 {1/3, 1/18, 1/36}; D3Q27 {8/27, 2/27, 1/54, 1/216}, each quotient
+// rounded once in the arithmetic type R (FP32, or FP64 as the reference's DP build)
+template <int Q, typename R = float>
+__host__ __device__ constexpr R lat_w(int l) {
+    return Q == 19 ? (lat_speed2(l) == 0 ? R(1) / R(3) : lat_speed2(l) == 1 ? R(1) / R(18) : R(1) / R(36))
+                   : (lat_speed2(l) == 0 ? R(8) / R(27)
+                      : lat_speed2(l) == 1 ? R(2) / R(27)
+                      : lat_speed2(l) == 2 ? R(1) / R(54)
+                                           : R(1) / R(216));
 }
+// tiny(1.0) of the arithmetic type: the smallest positive normal number
+template <typename R>
+__host__ __device__ constexpr R lat_tiny();
+template <>
+__host__ __device__ constexpr float lat_tiny<float>() { return 1.17549435e-38f; }
+template <>
+__host__ __device__ constexpr double lat_tiny<double>() { return 2.2250738585072014e-308; }
+// square root and maximum in the arithmetic type (sqrtf / fmaxf for FP32)
+__device__ __forceinline__ float real_sqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ double real_sqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float real_max(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double real_max(double a, double b) { return fmax(a, b); }
 __host__ __device__ constexpr int lat_opposite(int l) { return l == 0 ? 0 : ((l & 1) ? l + 1 : l - 1); }
 // index of direction (x,y,z) among the first Q directions, -1 if absent
 template <int Q>

@@ -14,53 +14,52 @@ namespace lbm {
 
 
 // Equilibrium offsets feq_l - w_l (m_fequil3_kernel.F90:112-167 in closed form).
-template <int Q>
-__device__ __forceinline__ void equilibrium(float (&fe)[Q], float drho, float rho, float ux, float uy, float uz,
-                                            bool cubic) {
-    const float usq = ux * ux + uy * uy + uz * uz;
-    const float R45 = 4.5f * rho;
-    const float R45o = cubic ? R45 : 0.0f;
-    const float A0 = drho - 1.5f * rho * usq;
-    const float B0 = 3.0f * rho - (cubic ? R45 * usq : 0.0f);
-    fe[0] = lat_w<Q>(0) * A0;
+template <int Q, typename R>
+__device__ __forceinline__ void equilibrium(R (&fe)[Q], R drho, R rho, R ux, R uy, R uz, bool cubic) {
+    const R usq = ux * ux + uy * uy + uz * uz;
+    const R R45 = R(4.5) * rho;
+    const R R45o = cubic ? R45 : R(0.0);
+    const R A0 = drho - R(1.5) * rho * usq;
+    const R B0 = R(3.0) * rho - (cubic ? R45 * usq : R(0.0));
+    fe[0] = lat_w<Q, R>(0) * A0;
 #pragma unroll
     for (int l = 1; l < Q; l += 2) {
-        const float w = lat_w<Q>(l);
-        const float cu = cdot(lat_cx(l), lat_cy(l), lat_cz(l), ux, uy, uz);
-        const float cu2 = cu * cu;
-        const float E = w * (A0 + R45 * cu2);
-        const float O = w * cu * (B0 + R45o * cu2);
+        const R w = lat_w<Q, R>(l);
+        const R cu = cdot(lat_cx(l), lat_cy(l), lat_cz(l), ux, uy, uz);
+        const R cu2 = cu * cu;
+        const R E = w * (A0 + R45 * cu2);
+        const R O = w * cu * (B0 + R45o * cu2);
         fe[l] = E + O;
         fe[l + 1] = E - O;
     }
 }
 
 // Regularized non-equilibrium R(fneq) from a2 = sum H2 fneq (all l, including rest).
-template <int Q>
-__device__ __forceinline__ void regularized(float (&out)[Q], const Moments& m, float ux, float uy, float uz) {
-    const float third = 1.0f / 3.0f;
-    const float axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
-    const float axy = m.pxy, axz = m.pxz, ayz = m.pyz;
-    const float tr = axx + ayy + azz;
-    const float vx = axx * ux + axy * uy + axz * uz;
-    const float vy = axy * ux + ayy * uy + ayz * uz;
-    const float vz = axz * ux + ayz * uy + azz * uz;
-    out[0] = lat_w<Q>(0) * 4.5f * (-tr * third);
+template <int Q, typename R>
+__device__ __forceinline__ void regularized(R (&out)[Q], const MomentsT<R>& m, R ux, R uy, R uz) {
+    const R third = R(1.0) / R(3.0);
+    const R axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
+    const R axy = m.pxy, axz = m.pxz, ayz = m.pyz;
+    const R tr = axx + ayy + azz;
+    const R vx = axx * ux + axy * uy + axz * uz;
+    const R vy = axy * ux + ayy * uy + ayz * uz;
+    const R vz = axz * ux + ayz * uy + azz * uz;
+    out[0] = lat_w<Q, R>(0) * R(4.5) * (-tr * third);
 #pragma unroll
     for (int l = 1; l < Q; l += 2) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-        const float w = 4.5f * lat_w<Q>(l);
-        const float cu = cdot(cx, cy, cz, ux, uy, uz);
-        float cac = 0.f;
+        const R w = R(4.5) * lat_w<Q, R>(l);
+        const R cu = cdot(cx, cy, cz, ux, uy, uz);
+        R cac = R(0);
         macc(cac, cx * cx, axx);
         macc(cac, cy * cy, ayy);
         macc(cac, cz * cz, azz);
-        macc(cac, cx * cy, 2.0f * axy);
-        macc(cac, cx * cz, 2.0f * axz);
-        macc(cac, cy * cz, 2.0f * ayz);
-        const float cau = cdot(cx, cy, cz, vx, vy, vz);
-        const float E = w * (cac - tr * third);
-        const float O = w * (cu * (3.0f * cac - tr) - 2.0f * cau);
+        macc(cac, cx * cy, R(2.0) * axy);
+        macc(cac, cx * cz, R(2.0) * axz);
+        macc(cac, cy * cz, R(2.0) * ayz);
+        const R cau = cdot(cx, cy, cz, vx, vy, vz);
+        const R E = w * (cac - tr * third);
+        const R O = w * (cu * (R(3.0) * cac - tr) - R(2.0) * cau);
         out[l] = E + O;
         out[l + 1] = E - O;
     }
@@ -68,13 +67,13 @@ __device__ __forceinline__ void regularized(float (&out)[Q], const Moments& m, f
 
 // Row-chunk staging: cells [i0, i0+n) of row (j,k), n <= 128.
 #define TILE_ILP 8
-template <int Q>
-__device__ __forceinline__ void tile_load(float* __restrict__ sm, const float* __restrict__ f, long long cell0, int n) {
+template <int Q, typename R>
+__device__ __forceinline__ void tile_load(R* __restrict__ sm, const R* __restrict__ f, long long cell0, int n) {
     // TILE_ILP independent loads in flight per thread before their shared-memory stores
-    const float* src = f + cell0 * Q;
+    const R* src = f + cell0 * Q;
     const int m = n * Q, step = blockDim.x * TILE_ILP;
     for (int e0 = threadIdx.x; e0 < m; e0 += step) {
-        float v[TILE_ILP];
+        R v[TILE_ILP];
 #pragma unroll
         for (int u = 0; u < TILE_ILP; ++u) {
             const int e = e0 + u * blockDim.x;
@@ -87,39 +86,39 @@ __device__ __forceinline__ void tile_load(float* __restrict__ sm, const float* _
         }
     }
 }
-template <int Q>
-__device__ __forceinline__ void tile_store(const float* __restrict__ sm, float* __restrict__ f, long long cell0, int n) {
-    float* dst = f + cell0 * Q;
+template <int Q, typename R>
+__device__ __forceinline__ void tile_store(const R* __restrict__ sm, R* __restrict__ f, long long cell0, int n) {
+    R* dst = f + cell0 * Q;
     const int m = n * Q;
     for (int e = threadIdx.x; e < m; e += blockDim.x) dst[e] = sm[e];
 }
 
 // fequil3: feq on interior cells (m_fequil3_kernel.F90:7-123)
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_fequil3(float* feq, const float* rho, const float* u, const float* v,
-                                                     const float* w, RefGrid g, int ibgk) {
-    __shared__ float sm[128 * Q];
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_fequil3(R* feq, const R* rho, const R* u, const R* v,
+                                                     const R* w, RefGrid g, int ibgk) {
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     const int n = min(128, g.nx + 1 - i0);
     const int t = threadIdx.x;
     if (n <= 0) return;
     if (t < n) {
         const long long c = g.cell(i0 + t, j, k);
-        float fe[Q];
-        equilibrium<Q>(fe, rho[c] - 1.0f, rho[c], u[c], v[c], w[c], ibgk == 3);
+        R fe[Q];
+        equilibrium<Q>(fe, rho[c] - R(1.0), rho[c], u[c], v[c], w[c], ibgk == 3);
 #pragma unroll
-        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fe[l] + lat_w<Q>(l);
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fe[l] + lat_w<Q, R>(l);
     }
     __syncthreads();
     tile_store<Q>(sm, feq, g.cell(i0, j, k), n);
 }
 
 // postcoll: collide interior cells in place with the given moments (m_postcoll_kernel.F90:7-255)
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, const float* rho, const float* u,
-                                                      const float* v, const float* w, const float* abl, RefGrid g,
-                                                      CollideParams cp) {
-    __shared__ float sm[128 * Q];
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_postcoll(R* f, R* tau, const R* rho, const R* u,
+                                                      const R* v, const R* w, const R* abl, RefGrid g,
+                                                      CollideParamsT<R> cp) {
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     const int n = min(128, g.nx + 1 - i0);
     const int t = threadIdx.x;
@@ -128,19 +127,19 @@ __global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, cons
     __syncthreads();
     if (t < n) {
         const long long c = g.cell(i0 + t, j, k);
-        float fp[Q];
+        R fp[Q];
 #pragma unroll
-        for (int l = 0; l < Q; ++l) fp[l] = sm[t * Q + l] - lat_w<Q>(l);
-        const Moments m = moments<Q>(fp);
-        const float r = rho[c];
-        TurbIn tb;
+        for (int l = 0; l < Q; ++l) fp[l] = sm[t * Q + l] - lat_w<Q, R>(l);
+        const MomentsT<R> m = moments<Q>(fp);
+        const R r = rho[c];
+        TurbInT<R> tb;
         tb.on = false;
-        tb.dux = tb.duy = tb.duz = 0.f;
-        const float tnew = collide<Q>(fp, m, r - 1.0f, r, u[c], v[c], w[c], cp, abl ? abl[k - 1] : 0.0f, tau[c],
+        tb.dux = tb.duy = tb.duz = R(0);
+        const R tnew = collide<Q>(fp, m, r - R(1.0), r, u[c], v[c], w[c], cp, abl ? abl[k - 1] : R(0.0), tau[c],
                                       false, tb);
         if (cp.ivreman) tau[c] = tnew;
 #pragma unroll
-        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fp[l] + lat_w<Q>(l);
+        for (int l = 0; l < Q; ++l) sm[t * Q + l] = fp[l] + lat_w<Q, R>(l);
     }
     __syncthreads();
     tile_store<Q>(sm, f, g.cell(i0, j, k), n);
@@ -153,8 +152,8 @@ __global__ void __launch_bounds__(128) k_ref_postcoll(float* f, float* tau, cons
 // read would serialise over the different l of a warp).  Each thread keeps
 // DRIFT_ILP loads in flight before its stores.
 #define DRIFT_ILP 4
-template <int Q>
-__global__ void __launch_bounds__(256) k_ref_drift(float* __restrict__ f, const float* __restrict__ feq, RefGrid g) {
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(256) k_ref_drift(R* __restrict__ f, const R* __restrict__ feq, RefGrid g) {
     // one block per interior row (j,k), looping over its nx*Q outputs
     __shared__ long long sd[Q];
     if (threadIdx.x < Q) {
@@ -167,7 +166,7 @@ __global__ void __launch_bounds__(256) k_ref_drift(float* __restrict__ f, const 
     const long long base = g.cell(1, j, k) * Q;
     const int n = Q * g.nx;
     for (int e0 = threadIdx.x; e0 < n; e0 += blockDim.x * DRIFT_ILP) {
-        float v[DRIFT_ILP];
+        R v[DRIFT_ILP];
 #pragma unroll
         for (int u = 0; u < DRIFT_ILP; ++u) {
             const int e = e0 + u * blockDim.x;
@@ -182,10 +181,10 @@ __global__ void __launch_bounds__(256) k_ref_drift(float* __restrict__ f, const 
 }
 
 // macrovars over the ghost-inclusive grid, summation order of m_macrovars_kernel.F90:175-187
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_macrovars(float* rho, float* u, float* v, float* w, const float* f,
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_macrovars(R* rho, R* u, R* v, R* w, const R* f,
                                                        RefGrid g) {
-    __shared__ float sm[128 * Q];
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128, j = blockIdx.y, k = blockIdx.z;
     const int n = min(128, g.nx + 2 - i0);
     const int t = threadIdx.x;
@@ -193,16 +192,16 @@ __global__ void __launch_bounds__(128) k_ref_macrovars(float* rho, float* u, flo
     tile_load<Q>(sm, f, g.cell(i0, j, k), n);
     __syncthreads();
     if (t < n) {
-        float tr = 0.f, tu = 0.f, tv = 0.f, tw = 0.f;
+        R tr = R(0), tu = R(0), tv = R(0), tw = R(0);
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
-            const float tf = sm[t * Q + l];
+            const R tf = sm[t * Q + l];
             tr = tr + tf;
             macc(tu, lat_cx(l), tf);
             macc(tv, lat_cy(l), tf);
             macc(tw, lat_cz(l), tf);
         }
-        const float inv = 1.0f / tr;
+        const R inv = R(1.0) / tr;
         const long long c = g.cell(i0 + t, j, k);
         rho[c] = tr;
         u[c] = tu * inv;
@@ -212,10 +211,10 @@ __global__ void __launch_bounds__(128) k_ref_macrovars(float* rho, float* u, flo
 }
 
 // regularization: f = R(f - feq) on interior cells (m_regularization_kernel.F90:6-122)
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_regularization(float* f, const float* feq, const float* u,
-                                                            const float* v, const float* w, RefGrid g) {
-    __shared__ float sm[128 * Q];
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_regularization(R* f, const R* feq, const R* u,
+                                                            const R* v, const R* w, RefGrid g) {
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     const int n = min(128, g.nx + 1 - i0);
     const int t = threadIdx.x;
@@ -224,11 +223,11 @@ __global__ void __launch_bounds__(128) k_ref_regularization(float* f, const floa
     __syncthreads();
     if (t < n) {
         const long long c = g.cell(i0 + t, j, k);
-        float fn[Q];
+        R fn[Q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) fn[l] = sm[t * Q + l] - feq[c * Q + l];
-        const Moments m = moments<Q>(fn);
-        float out[Q];
+        const MomentsT<R> m = moments<Q>(fn);
+        R out[Q];
         regularized<Q>(out, m, u[c], v[c], w[c]);
 #pragma unroll
         for (int l = 0; l < Q; ++l) sm[t * Q + l] = out[l];
@@ -239,9 +238,9 @@ __global__ void __launch_bounds__(128) k_ref_regularization(float* f, const floa
 
 // vreman: tau from a non-equilibrium f with the standalone guards
 // (alphamag and beta start at 1e-5, no ablvisc; m_vreman_kernel.F90:281-325)
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_vreman(const float* f, float* tau, RefGrid g, CollideParams cp) {
-    __shared__ float sm[128 * Q];
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_vreman(const R* f, R* tau, RefGrid g, CollideParamsT<R> cp) {
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     const int n = min(128, g.nx + 1 - i0);
     const int t = threadIdx.x;
@@ -249,45 +248,46 @@ __global__ void __launch_bounds__(128) k_ref_vreman(const float* f, float* tau, 
     tile_load<Q>(sm, f, g.cell(i0, j, k), n);
     __syncthreads();
     if (t < n) {
-        float fn[Q];
+        R fn[Q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) fn[l] = sm[t * Q + l];
-        const Moments m = moments<Q>(fn);
-        const float third = 1.0f / 3.0f;
-        const float axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
-        const float axy = m.pxy, axz = m.pxz, ayz = m.pyz;
-        const float g0 = 0.00001f;
-        const float amag = g0 + (axx * axx + ayy * ayy + azz * azz + 2.0f * (axy * axy + axz * axz + ayz * ayz));
-        const float b11 = g0 + axx * axx + axy * axy + axz * axz;
-        const float b22 = g0 + axy * axy + ayy * ayy + ayz * ayz;
-        const float b33 = g0 + axz * axz + ayz * ayz + azz * azz;
-        const float b12 = g0 + axx * axy + axy * ayy + axz * ayz;
-        const float b13 = g0 + axx * axz + axy * ayz + axz * azz;
-        const float b23 = g0 + axy * axz + ayy * ayz + ayz * azz;
-        const float bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
-        const float tt = bb / amag;
-        const float nut = (tt > cp.eps) ? cp.cvre * sqrtf(tt) : 0.0f;
-        tau[g.cell(i0 + t, j, k)] = 3.0f * (cp.kinevisc + nut) + 0.5f;
+        const MomentsT<R> m = moments<Q>(fn);
+        const R third = R(1.0) / R(3.0);
+        const R axx = m.pxx - m.s0 * third, ayy = m.pyy - m.s0 * third, azz = m.pzz - m.s0 * third;
+        const R axy = m.pxy, axz = m.pxz, ayz = m.pyz;
+        const R g0 = R(0.00001);
+        const R amag = g0 + (axx * axx + ayy * ayy + azz * azz + R(2.0) * (axy * axy + axz * axz + ayz * ayz));
+        const R b11 = g0 + axx * axx + axy * axy + axz * axz;
+        const R b22 = g0 + axy * axy + ayy * ayy + ayz * ayz;
+        const R b33 = g0 + axz * axz + ayz * ayz + azz * azz;
+        const R b12 = g0 + axx * axy + axy * ayy + axz * ayz;
+        const R b13 = g0 + axx * axz + axy * ayz + axz * azz;
+        const R b23 = g0 + axy * axz + ayy * ayz + ayz * azz;
+        const R bb = b11 * b22 - b12 * b12 + b11 * b33 - b13 * b13 + b22 * b33 - b23 * b23;
+        const R tt = bb / amag;
+        const R nut = (tt > cp.eps) ? cp.cvre * real_sqrt(tt) : R(0.0);
+        tau[g.cell(i0 + t, j, k)] = R(3.0) * (cp.kinevisc + nut) + R(0.5);
     }
 }
 
 // compute_fneq / compute_f: elementwise over every element, ghosts included
-__global__ void k_ref_axpy(float* f, const float* feq, long long n, float sgn) {
+template <typename R = float>
+__global__ void k_ref_axpy(R* f, const R* feq, long long n, int sgn) {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
-        f[e] = (sgn > 0.f) ? (feq[e] + f[e]) : (f[e] - feq[e]);
+        f[e] = (sgn > 0) ? (feq[e] + f[e]) : (f[e] - feq[e]);
 }
 
 // solids: swap pairs (l,l+1), l = 2,4,..,nl-1 (1-based) at blanked interior cells (m_solids.F90:24-36)
-template <int Q>
-__global__ void k_ref_solids(float* f, const int32_t* blank, RefGrid g) {
+template <int Q, typename R = float>
+__global__ void k_ref_solids(R* f, const int32_t* blank, RefGrid g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     if (i > g.nx) return;
     const long long c = g.cell(i, j, k);
     if (blank[c] == 0) return;
-    float* p = f + c * Q;
+    R* p = f + c * Q;
 #pragma unroll
     for (int l = 1; l + 1 < Q; l += 2) {
-        const float a = p[l];
+        const R a = p[l];
         p[l] = p[l + 1];
         p[l + 1] = a;
     }
@@ -296,10 +296,10 @@ __global__ void k_ref_solids(float* f, const int32_t* blank, RefGrid g) {
 // forcings_apply: f += feq2(rho, u - F/rho) - feq2(rho, u) at interior cells with
 // rho > 0 (m_forcings_apply_kernel.F90:47-213; second-order equilibria), in the
 // closed form w rho [3 dcu + 4.5 dcu (2 cu + dcu) - 1.5 (2 u.du + du.du)].
-template <int Q>
-__global__ void __launch_bounds__(128) k_ref_forcings_apply(float* f, const float* force, const float* rho,
-                                                            const float* u, const float* v, const float* w, RefGrid g) {
-    __shared__ float sm[128 * Q];
+template <int Q, typename R = float>
+__global__ void __launch_bounds__(128) k_ref_forcings_apply(R* f, const R* force, const R* rho,
+                                                            const R* u, const R* v, const R* w, RefGrid g) {
+    __shared__ R sm[128 * Q];
     const int i0 = blockIdx.x * 128 + 1, j = blockIdx.y + 1, k = blockIdx.z + 1;
     const int n = min(128, g.nx + 1 - i0);
     const int t = threadIdx.x;
@@ -308,21 +308,21 @@ __global__ void __launch_bounds__(128) k_ref_forcings_apply(float* f, const floa
     __syncthreads();
     if (t < n) {
         const long long c = g.cell(i0 + t, j, k);
-        const float rr = rho[c];
-        if (rr > 0.0f) {
-            const float ux = u[c], uy = v[c], uz = w[c];
-            const float dux = -force[3 * c] / rr, duy = -force[3 * c + 1] / rr, duz = -force[3 * c + 2] / rr;
-            const float dusq = dux * (2.0f * ux + dux) + duy * (2.0f * uy + duy) + duz * (2.0f * uz + duz);
-            float* p = sm + t * Q;
-            p[0] += lat_w<Q>(0) * rr * (-1.5f * dusq);
+        const R rr = rho[c];
+        if (rr > R(0.0)) {
+            const R ux = u[c], uy = v[c], uz = w[c];
+            const R dux = -force[3 * c] / rr, duy = -force[3 * c + 1] / rr, duz = -force[3 * c + 2] / rr;
+            const R dusq = dux * (R(2.0) * ux + dux) + duy * (R(2.0) * uy + duy) + duz * (R(2.0) * uz + duz);
+            R* p = sm + t * Q;
+            p[0] += lat_w<Q, R>(0) * rr * (-R(1.5) * dusq);
 #pragma unroll
             for (int l = 1; l < Q; l += 2) {
                 const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-                const float cu = cdot(cx, cy, cz, ux, uy, uz);
-                const float dcu = cdot(cx, cy, cz, dux, duy, duz);
-                const float wr = lat_w<Q>(l) * rr;
-                const float dE = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
-                const float dO = wr * 3.0f * dcu;
+                const R cu = cdot(cx, cy, cz, ux, uy, uz);
+                const R dcu = cdot(cx, cy, cz, dux, duy, duz);
+                const R wr = lat_w<Q, R>(l) * rr;
+                const R dE = wr * (R(4.5) * dcu * (R(2.0) * cu + dcu) - R(1.5) * dusq);
+                const R dO = wr * R(3.0) * dcu;
                 p[l] += dE + dO;
                 p[l + 1] += dE - dO;
             }
@@ -334,41 +334,42 @@ __global__ void __launch_bounds__(128) k_ref_forcings_apply(float* f, const floa
 
 // inflow_turbulence_forcing: df(l,j,k) = feq(rho,u+ampl*uu) - feq(rho,u) at i = iturb
 // (m_inflow_turbulence_forcing.F90:44-128), evaluated as a difference of offsets
-template <int Q>
-__global__ void k_ref_turb_forcing(float* df, const float* rho, const float* u, const float* v, const float* w,
-                                   const float* uu, const float* vv, const float* ww, float ampl, int lit, int ip,
+template <int Q, typename R = float>
+__global__ void k_ref_turb_forcing(R* df, const R* rho, const R* u, const R* v, const R* w,
+                                   const R* uu, const R* vv, const R* ww, R ampl, int lit, int ip,
                                    int ibgk, RefGrid g) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x + 1, k = blockIdx.y + 1;
     if (j > g.ny) return;
     const long long c = g.cell(ip, j, k);
     const long long t = (long long)(j - 1) + (long long)g.ny * ((long long)(k - 1) + (long long)g.nz * lit);
-    const float r = rho[c];
-    const float ux = u[c], uy = v[c], uz = w[c];
-    const float dux = ampl * uu[t], duy = ampl * vv[t], duz = ampl * ww[t];
+    const R r = rho[c];
+    const R ux = u[c], uy = v[c], uz = w[c];
+    const R dux = ampl * uu[t], duy = ampl * vv[t], duz = ampl * ww[t];
     const bool cubic = ibgk == 3;
-    const float usq = ux * ux + uy * uy + uz * uz;
-    const float dusq = dux * (2.0f * ux + dux) + duy * (2.0f * uy + duy) + duz * (2.0f * uz + duz);
-    const float usq2 = usq + dusq;
-    float* o = df + ((long long)(j - 1) + (long long)g.ny * (k - 1)) * Q;
-    o[0] = lat_w<Q>(0) * r * (-1.5f * dusq);
+    const R usq = ux * ux + uy * uy + uz * uz;
+    const R dusq = dux * (R(2.0) * ux + dux) + duy * (R(2.0) * uy + duy) + duz * (R(2.0) * uz + duz);
+    const R usq2 = usq + dusq;
+    R* o = df + ((long long)(j - 1) + (long long)g.ny * (k - 1)) * Q;
+    o[0] = lat_w<Q, R>(0) * r * (-R(1.5) * dusq);
 #pragma unroll
     for (int l = 1; l < Q; l += 2) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-        const float wr = lat_w<Q>(l) * r;
-        const float cu = cdot(cx, cy, cz, ux, uy, uz);
-        const float dcu = cdot(cx, cy, cz, dux, duy, duz);
-        const float cun = cu + dcu;
-        const float E = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
-        float od = 3.0f * dcu;
-        if (cubic) od += 4.5f * dcu * (cun * cun + cun * cu + cu * cu - usq2) - 4.5f * cu * dusq;
-        const float O = wr * od;
+        const R wr = lat_w<Q, R>(l) * r;
+        const R cu = cdot(cx, cy, cz, ux, uy, uz);
+        const R dcu = cdot(cx, cy, cz, dux, duy, duz);
+        const R cun = cu + dcu;
+        const R E = wr * (R(4.5) * dcu * (R(2.0) * cu + dcu) - R(1.5) * dusq);
+        R od = R(3.0) * dcu;
+        if (cubic) od += R(4.5) * dcu * (cun * cun + cun * cu + cu * cu - usq2) - R(4.5) * cu * dusq;
+        const R O = wr * od;
         o[l] = E + O;
         o[l + 1] = E - O;
     }
 }
 
 // inflow_turbulence_apply: f(l,ip,j,k) += df(l,j,k) (m_inflow_turbulence_apply.F90:19-28)
-__global__ void k_ref_turb_apply(float* f, const float* df, int ip, RefGrid g) {
+template <typename R = float>
+__global__ void k_ref_turb_apply(R* f, const R* df, int ip, RefGrid g) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;   // over (l, j)
     const int k = blockIdx.y + 1;
     const int nl = g.nl;
@@ -378,14 +379,15 @@ __global__ void k_ref_turb_apply(float* f, const float* df, int ip, RefGrid g) {
 }
 
 // fillghosts: ghost cells copy the nearest interior cell (m_fillghosts.F90:18-29)
-__global__ void k_ref_fillghosts(float* f, RefGrid g) {
+template <typename R = float>
+__global__ void k_ref_fillghosts(R* f, RefGrid g) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
     if (i > g.nx + 1) return;
     const int i1 = min(max(i, 1), g.nx), j1 = min(max(j, 1), g.ny), k1 = min(max(k, 1), g.nz);
     if (i1 == i && j1 == j && k1 == k) return;
     const int nl = g.nl;
-    const float* s = f + g.cell(i1, j1, k1) * nl;
-    float* d = f + g.cell(i, j, k) * nl;
+    const R* s = f + g.cell(i1, j1, k1) * nl;
+    R* d = f + g.cell(i, j, k) * nl;
     for (int l = 0; l < nl; ++l) d[l] = s[l];
 }
 
