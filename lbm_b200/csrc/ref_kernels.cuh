@@ -1,11 +1,15 @@
 // ref_kernels.cuh -- per-call kernels on the reference layout
 // f(nl,0:nx+1,0:ny+1,0:nz+1) (l fastest), one per reference subroutine.
 //
-// Cell-wise kernels stage a row chunk of 128 cells (128*nl contiguous floats)
+// Cell-wise kernels stage a row chunk of 128 cells (128*nl contiguous values)
 // through shared memory, so the global reads and writes are coalesced even
 // though each cell's nl populations are contiguous; the per-cell math reads
 // the staged values with an odd stride (nl = 19 or 27), free of bank
-// conflicts.
+// conflicts for FP32.
+//
+// Every kernel takes the arithmetic type R as a template argument: float for
+// the reference's default build, double for its DP build (the _f64 entry
+// points), where -r8 makes every real, tiny() and eps double precision.
 #pragma once
 
 #include "collide.cuh"
