@@ -25,10 +25,15 @@ from .api import Lbm, Params
 class ProbeProblem:
     """u at probe cells after ``nsteps`` steps, and the reverse sweep of its loss.
 
-    probes: int array (P, 3) of 1-based interior (i, j, k) cells."""
+    probes: int array (P, 3) of 1-based interior (i, j, k) cells.  dtype
+    torch.float64 runs the forward through the FP64 entry points (the
+    reference's DP build), for finite-difference checks; the reverse sweep
+    runs on FP32 states."""
 
-    def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10):
+    def __init__(self, params: Params, probes, nsteps: int, blanking=None, checkpoint: int = 10,
+                 dtype=torch.float32):
         self.p = params
+        self.dtype = dtype
         self.lbm = Lbm(params)
         self.nsteps = int(nsteps)
         self.K = max(1, int(checkpoint))
@@ -37,13 +42,13 @@ class ProbeProblem:
         self.probes = pr
         # flat indices into the (nz+2, ny+2, nx+2) scalar fields
         self.pidx = torch.from_numpy((pr[:, 2] * (params.ny + 2) + pr[:, 1]) * (params.nx + 2) + pr[:, 0]).cuda()
-        self.tau = torch.full(params.sshape, 3.0 * params.kinevisc + 0.5, dtype=torch.float32, device="cuda")
+        self.tau = torch.full(params.sshape, 3.0 * params.kinevisc + 0.5, dtype=dtype, device="cuda")
         self.ckpt = {}
 
     # ---- forward ----------------------------------------------------------------------
     def _macro(self, f):
         L = self.lbm
-        R = [L.empty_s() for _ in range(4)]
+        R = [L.empty_s(self.dtype) for _ in range(4)]
         L.macrovars(*R, f)
         return R
 
@@ -77,6 +82,8 @@ class ProbeProblem:
     # ---- reverse ----------------------------------------------------------------------
     def backward(self, uhat_probes):
         """Adjoint of the probe velocities (P, 3) -> (d loss / d f1 initial, d loss / d uvel)."""
+        if self.dtype != torch.float32:
+            raise ValueError("the reverse sweep runs on FP32 states; this problem's forward is %s" % self.dtype)
         L = self.lbm
         Ah, Bh = L.empty_f(), L.empty_f()
         Rh = [L.empty_s() for _ in range(4)]

@@ -378,3 +378,54 @@ def test_state_layout_sweep_refuses_unsupported_states():
     a, b = L.empty_state(), L.empty_state()
     with pytest.raises(LbmError, match="ihrr"):
         L.state_adjoint_step(a, b, a.clone(), True, torch.zeros(6, device="cuda"))
+
+
+def test_full_size_gradient_matches_fp64_gpu_finite_differences():
+    """The adjoint workload at its own size: D3Q19 256x128x128, sphere r = 16,
+    200 probes, 100 steps, checkpoints every 10.  The state-layout sweep's
+    gradient (FP32 fused forward) against central differences of the FP64
+    forward run on the GPU through the _f64 entry points (the reference's DP
+    build), along 8 seeded directions (4 in f1, 4 in uvel), each within 1e-4."""
+    from lbm_b200 import Params
+    from lbm_b200.adjoint import FusedProbeProblem, ProbeProblem, initial_state
+    wl = W.ADJOINT_Q19
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=10,
+               kinevisc=wl.kinevisc)
+    blank = torch.from_numpy(W.blanking(wl)).cuda()
+    probes = W.probe_cells(wl, 200, 0)
+    spin = ProbeProblem(p, probes, wl.steps, blanking=blank, checkpoint=10)
+    rho, u, v, w = (torch.from_numpy(x).cuda() for x in W.initial_macro(wl))
+    uvel = torch.from_numpy(W.inflow_profile(wl)).cuda()
+    f1, f2 = initial_state(spin.lbm, rho, u, v, w, uvel)
+    R = spin._macro(f1)
+    for _ in range(20):                       # leave the exact initial equilibrium
+        f1, f2 = spin._step(f1, f2, R, uvel)
+    spin.close()
+    p64 = ProbeProblem(p, probes, wl.steps, blanking=blank, dtype=torch.float64)
+    F1, F2, U = f1.double(), f2.double(), uvel.double()
+    dU = torch.from_numpy(W.inflow_perturbation(wl.nz, 0, 5e-3)).cuda().double()
+    T = p64.forward(F1, F2, U + dU, keep=False)
+    u64 = p64.forward(F1, F2, U, keep=False)
+    fb = FusedProbeProblem(p, probes, wl.steps, blanking=blank, checkpoint=10)
+    fb.forward(f1, f2, uvel)
+    gf, gu = (t.double() for t in fb.backward((2.0 * (u64 - T)).float()))
+    fb.close()
+
+    def loss(a, b):
+        return float(((p64.forward(a, F2, b, keep=False) - T) ** 2).sum())
+
+    gen = torch.Generator(device="cuda").manual_seed(44)
+    inner = (slice(1, -1),) * 3
+    worst = 0.0
+    for d in range(8):
+        df, du = torch.zeros_like(F1), torch.zeros_like(U)
+        if d < 4:
+            df[inner] = 1e-6 * torch.randn(df[inner].shape, generator=gen, device="cuda", dtype=torch.float64)
+        else:
+            du = 1e-6 * torch.randn(U.shape, generator=gen, device="cuda", dtype=torch.float64)
+        fd = (loss(F1 + df, U + du) - loss(F1 - df, U - du)) / 2.0
+        ad = float((gf * df).sum() + (gu * du).sum())
+        worst = max(worst, rel(fd, ad))
+        assert rel(fd, ad) < 1e-4, (d, fd, ad)
+    print("worst relative error of 8 directional derivatives at 256x128x128:", worst)
+    p64.close()
