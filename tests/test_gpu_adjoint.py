@@ -4,7 +4,8 @@ Each adjoint kernel passes a dot-product test, <y^, J x> = <J^T y^, x>, with
 J x from central differences of the FP64 oracle's forward kernel.  The full
 sweep's gradient of a probe-misfit loss matches central differences of the
 FP64 oracle's time loop along 8 seeded directions (4 in the initial f, 4 in
-the inflow profile) to a relative 1e-4."""
+the inflow profile) to a relative 1e-4; at the adjoint workload's full size
+the central differences come from the FP64 forward run on the GPU."""
 import numpy as np
 import pytest
 
