@@ -57,6 +57,9 @@ def parse():
                          "against one fused forward step, on a resident state (about 2.5 GB)")
     ap.add_argument("--accuracy", action="store_true",
                     help="FP16-offset storage error study (city workload) instead of the timing run")
+    ap.add_argument("--per-call", action="store_true",
+                    help="main.F90's step through the per-call entry points (reference layout) on the workload, "
+                         "FP32 and FP64 (the reference's DP build)")
     return ap.parse_args()
 
 
@@ -676,6 +679,74 @@ def adjoint_step_bench(a):
     return 0
 
 
+def per_call_bench(a):
+    """MLUPS of main.F90's step (main.F90:283-329) made of the per-call entry
+    points on reference-layout arrays: inflow-turbulence forcing, postcoll,
+    turbulence apply, boundarycond, drift, macrovars.  This is the path a
+    Fortran driver gets by switching its calls one by one; the FP64 arm is the
+    DP build's (the _f64 entry points)."""
+    import torch
+    from lbm_b200 import Lbm, Params, workloads as W
+    from lbm_b200.adjoint import initial_state
+    torch.cuda.set_device(0)
+    wl = W.WORKLOADS[a.workload]
+    p = Params(nx=wl.nx, ny=wl.ny, nz=wl.nz, nl=wl.nl, ibnd=wl.ibnd, jbnd=wl.jbnd, kbnd=wl.kbnd, iturb_pos=10,
+               kinevisc=wl.kinevisc, smagorinsky=wl.smagorinsky)
+    out = {}
+    for name, dt in (("f32", torch.float32), ("f64", torch.float64)):
+        L = Lbm(p)
+        rho, u, v, w = (torch.from_numpy(x).cuda().to(dt) for x in W.initial_macro(wl))
+        uvel = torch.from_numpy(W.inflow_profile(wl)).cuda().to(dt)
+        f1, f2 = initial_state(L, rho, u, v, w, uvel)
+        L.macrovars(rho, u, v, w, f1)
+        tau = torch.full(p.sshape, 3.0 * wl.kinevisc + 0.5, dtype=dt, device="cuda")
+        turb = [torch.from_numpy(x).cuda().to(dt) for x in W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, wl.seed)]
+        df = torch.zeros((wl.nz, wl.ny, wl.nl), dtype=dt, device="cuda")
+        it = [0]
+
+        def step():
+            it[0] += 1
+            if wl.lturb:
+                L.inflow_turbulence_forcing(df, rho, u, v, w, *turb, wl.ampl, it[0], wl.nrturb)
+            L.postcoll(f1, tau, rho, u, v, w)
+            if wl.lturb:
+                L.inflow_turbulence_apply(f1, df)
+            L.boundarycond(f1, f2, uvel)
+            L.drift(f2, f1)
+            L.macrovars(rho, u, v, w, f2)
+
+        def swap_step():
+            nonlocal f1, f2
+            step()
+            f1, f2 = f2, f1
+
+        for _ in range(a.warmup):
+            swap_step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = L.launches
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            e0.record(L.stream)
+            for _ in range(a.steps):
+                swap_step()
+            e1.record(L.stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"value": round(wl.cells * a.steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS",
+                     "ms_per_step": round(ms / a.steps, 4), "gpu_launches": L.launches - n0,
+                     "status": L.status(), "clocks": clk.report()}
+        L.close()
+        del f1, f2, rho, u, v, w, tau, turb, df
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": "MLUPS of the per-call step (reference layout, main.F90:283-329)", "unit": "MLUPS",
+                      "value": out["f32"]["value"], "higher_is_better": True, "n_gpus": 1, "steps": a.steps,
+                      "warmup": a.warmup, "config": {"workload": wl.name, "grid": [wl.nx, wl.ny, wl.nz],
+                                                     "lattice": "D3Q%d" % wl.nl},
+                      "data": "synthetic (seeded initial field and turbulence fields)",
+                      "f32": out["f32"], "f64_dp_build": out["f64"]}))
+    return 0
+
+
 def slab_bench(a):
     """MLUPS of j slabs: each rank steps one tile of the default workload's size
     (weak scaling: the domain grows in j with the ranks) and exchanges its halo
@@ -745,6 +816,8 @@ def main():
     a = parse()
     if a.slabs and a.impl == "ours":
         return slab_bench(a)
+    if a.per_call and a.impl == "ours":
+        return per_call_bench(a)
     if a.adjoint_step and a.impl == "ours":
         return adjoint_step_bench(a)
     if a.adjoint and a.impl == "ours":

@@ -132,8 +132,8 @@ class ProbeProblem:
 
 def initial_state(lbm: Lbm, rho, u, v, w, uvel):
     """(f1, f2) as main.F90:243-247 initialises them: fequil3, fillghosts, f1 = f2,
-    boundarycond twice."""
-    fB = lbm.empty_f()
+    boundarycond twice (in the dtype of rho: float32, or float64 for the DP build)."""
+    fB = lbm.empty_f(rho.dtype)
     lbm.fequil3(fB, rho, u, v, w)
     lbm.fillghosts(fB)
     fA = fB.clone()
