@@ -18,7 +18,13 @@ class Solver:
     def __init__(self, params: Params, rho, u, v, w, uvel, blanking=None, turbulence=None, it0: int = 0,
                  fused: bool = True):
         """rho,u,v,w: CUDA float32 (nz+2,ny+2,nx+2); uvel: (nz,); blanking: int32 mask or None;
-        turbulence: (uu, vv, ww, nrturb, ampl) or None."""
+        turbulence: (uu, vv, ww, nrturb, ampl) or None.  With float64 arrays (and
+        fused=False) the run goes through the FP64 entry points, the reference's
+        DP build."""
+        dt = rho.dtype
+        if fused and dt != torch.float32:
+            raise ValueError("the fused state takes float32 arrays (FP32 or FP16-offset storage); "
+                             "a float64 run uses the per-call path (fused=False)")
         self.p = params
         self.lbm = Lbm(params)
         L = self.lbm
@@ -27,13 +33,13 @@ class Solver:
         self.blanking = blanking
         self.turbulence = turbulence
         self.fused = fused
-        fB = L.empty_f()
+        fB = L.empty_f(dt)
         L.fequil3(fB, self.rho, self.u, self.v, self.w)
         L.fillghosts(fB)
         fA = fB.clone()
         L.boundarycond(fB, fA, self.uvel)
         L.boundarycond(fA, fB, self.uvel)
-        self.tau = torch.full(params.sshape, 3.0 * params.kinevisc + 0.5, dtype=torch.float32, device="cuda")
+        self.tau = torch.full(params.sshape, 3.0 * params.kinevisc + 0.5, dtype=dt, device="cuda")
         self.it = it0
         if fused:
             L.state_import(fA, fB, self.rho, self.u, self.v, self.w, it=it0)
@@ -47,7 +53,7 @@ class Solver:
         else:
             self.f1, self.f2 = fA, fB
             if turbulence is not None:
-                self.df = torch.zeros((params.nz, params.ny, params.nl), dtype=torch.float32, device="cuda")
+                self.df = torch.zeros((params.nz, params.ny, params.nl), dtype=dt, device="cuda")
 
     # ---- fused path ------------------------------------------------------------
     def step(self, n: int = 1):
