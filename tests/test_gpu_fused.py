@@ -117,6 +117,28 @@ def test_small_step_matches_oracle(nl, fused):
 
 
 @pytest.mark.parametrize("nl", [19, 27])
+def test_dp_build_run_matches_fp64_oracle(nl):
+    """main.F90's init and 30 steps (solids, turbulence slice) through the FP64
+    entry points (Solver with float64 arrays, the reference's DP build) against
+    the FP64 oracle, within FP64 round-off."""
+    from lbm_b200 import Solver
+    wl = SMALL.with_(nl=nl)
+    blank = W.blanking(wl)
+    turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
+
+    def d(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda().double()
+
+    rho, u, v, w = (d(a) for a in W.initial_macro(wl))
+    s = Solver(params_of(wl, iturb_pos=5), rho, u, v, w, d(W.inflow_profile(wl, np.float64)), blanking=cuda(blank),
+               turbulence=(d(turb[0]), d(turb[1]), d(turb[2]), wl.nrturb, wl.ampl), fused=False)
+    s.step(wl.steps)
+    gpu = tuple(host(t) for t in (*s.state(), *s.macro()))
+    s.close()
+    compare(gpu, run_oracle(wl, wl.steps, np.float64, 5, blank, turb), 1e-12, "DP build")
+
+
+@pytest.mark.parametrize("nl", [19, 27])
 @pytest.mark.parametrize("storage", ["f32", "f16"])
 def test_tma_kernel_matches_pull_kernel(nl, storage):
     """The shared-memory-tile step kernel gives the pull kernel's results (round-off)."""
