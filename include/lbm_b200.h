@@ -24,7 +24,8 @@
  * stream-ordered on the context's stream (the legacy default stream unless
  * lbm_set_stream names another); entry points that return results to host
  * memory synchronise that stream.  Floating-point data is FP32, the
- * reference's default precision.
+ * reference's default precision, except in the _f64 entry points, which take
+ * the FP64 arrays of its DP build.
  */
 #ifndef LBM_B200_H
 #define LBM_B200_H
