@@ -11,8 +11,9 @@ The record layout is the one gfortran writes: the record's bytes between a
 leading and a trailing 4-byte length marker, split into subrecords of at most
 2**31 - 9 bytes when longer.  A subrecord's leading marker is negative when
 another subrecord follows, and its trailing marker is negative when another
-precedes it.  Reading also accepts 8-byte markers (``-frecord-marker=8``) and
-f stored in double precision (the reference's ``DP=1`` build).
+precedes it.  Reading also accepts 8-byte markers (``-frecord-marker=8``).  f is
+float32, or double precision in the reference's ``DP=1`` build: both are
+written and read, and the reader converts to the precision the caller asks for.
 """
 from __future__ import annotations
 
@@ -74,9 +75,13 @@ def read_record(fh) -> bytes:
             return b"".join(parts)
 
 
-def write_restart(path: str, f, nx: int, ny: int, nz: int, nl: int, max_sub: int = MAX_SUBRECORD) -> None:
-    """Write f (reference layout, C order (nz+2, ny+2, nx+2, nl), float32) as the reference does."""
-    a = np.ascontiguousarray(np.asarray(f, dtype=np.float32))
+def write_restart(path: str, f, nx: int, ny: int, nz: int, nl: int, max_sub: int = MAX_SUBRECORD,
+                  dtype=np.float32) -> None:
+    """Write f (reference layout, C order (nz+2, ny+2, nx+2, nl)) as the reference does:
+    float32, or dtype=np.float64 for the record of its DP build (real(8) f)."""
+    if np.dtype(dtype) not in (np.dtype(np.float32), np.dtype(np.float64)):
+        raise ValueError("restart payloads are float32 or float64, not %s" % np.dtype(dtype))
+    a = np.ascontiguousarray(np.asarray(f, dtype=dtype))
     if a.shape != (nz + 2, ny + 2, nx + 2, nl):
         raise ValueError("f has shape %s, expected %s" % (a.shape, (nz + 2, ny + 2, nx + 2, nl)))
     d = os.path.dirname(path)
@@ -90,9 +95,11 @@ def write_restart(path: str, f, nx: int, ny: int, nz: int, nl: int, max_sub: int
         write_record(fh, payload, max_sub)
 
 
-def read_restart(path: str, expect=None):
-    """(nx, ny, nz, nl, f float32 in C order (nz+2, ny+2, nx+2, nl)).  With ``expect``
-    = (nx, ny, nz, nl), other dimensions raise ValueError (the reference stops)."""
+def read_restart(path: str, expect=None, dtype=np.float32):
+    """(nx, ny, nz, nl, f in C order (nz+2, ny+2, nx+2, nl)) with f converted to
+    ``dtype`` (float32 for the fused state and the FP32 entry points, float64 for
+    the _f64 ones; either record precision is read).  With ``expect`` = (nx, ny,
+    nz, nl), other dimensions raise ValueError (the reference stops)."""
     with open(path, "rb") as fh:
         rec = read_record(fh)
     nx, ny, nz, nl = (int(x) for x in np.frombuffer(rec[:16], "<i4"))
@@ -103,10 +110,10 @@ def read_restart(path: str, expect=None):
     if body == 4 * n:
         f = np.frombuffer(rec, "<f4", count=n, offset=16)
     elif body == 8 * n:
-        f = np.frombuffer(rec, "<f8", count=n, offset=16).astype(np.float32)
+        f = np.frombuffer(rec, "<f8", count=n, offset=16)
     else:
         raise ValueError("restart record of %d bytes does not hold f for %s" % (len(rec), (nx, ny, nz, nl)))
-    return nx, ny, nz, nl, f.reshape(nz + 2, ny + 2, nx + 2, nl).copy()
+    return nx, ny, nz, nl, f.astype(dtype).reshape(nz + 2, ny + 2, nx + 2, nl)
 
 
 def save_state(lbm, path: str) -> None:

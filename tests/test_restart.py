@@ -53,6 +53,24 @@ def test_eight_byte_markers_and_double_precision(tmp_path):
     assert np.array_equal(out[4], f64.astype(np.float32))
 
 
+def test_double_precision_record_round_trip(tmp_path):
+    """The DP build's record (real(8) f) as written here: 8 bytes per value between
+    the markers, read back bit for bit as float64 and rounded once as float32."""
+    nx, ny, nz, nl = 3, 2, 2, 27
+    f64 = np.random.default_rng(2).standard_normal((nz + 2, ny + 2, nx + 2, nl))
+    p = tmp_path / "restart_0000_000003.uf"
+    R.write_restart(str(p), f64, nx, ny, nz, nl, dtype=np.float64)
+    raw = p.read_bytes()
+    n = 16 + f64.nbytes
+    assert len(raw) == n + 8 and np.frombuffer(raw[:4], "<i4")[0] == n
+    assert np.array_equal(np.frombuffer(raw[20:-4], "<f8"), f64.ravel())
+    out = R.read_restart(str(p), expect=(nx, ny, nz, nl), dtype=np.float64)
+    assert out[4].dtype == np.float64 and np.array_equal(out[4], f64)
+    assert np.array_equal(R.read_restart(str(p))[4], f64.astype(np.float32))
+    with pytest.raises(ValueError):
+        R.write_restart(str(p), f64, nx, ny, nz, nl, dtype=np.float16)
+
+
 def test_dimension_mismatch_and_corruption(tmp_path):
     nx, ny, nz, nl = 2, 2, 2, 27
     f = np.zeros((nz + 2, ny + 2, nx + 2, nl), np.float32)
