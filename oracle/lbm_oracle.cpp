@@ -2,8 +2,9 @@
 //
 // TEST INFRASTRUCTURE ONLY.  This file restates, routine by routine, the
 // arithmetic of geirev/LBM (src/*.F90) so that the CUDA library can be checked
-// against it.  Only tests/, __graft_entry__.smoke() and the CPU-baseline leg
-// of bench.py load it; the product library never does.
+// against it.  Only tests/, __graft_entry__.smoke() and the CPU legs of
+// bench.py (the CPU baseline and the reference arm) load it; the product
+// library never does.
 //
 // Parity status: UNPINNED against reference outputs (the reference ships no
 // golden vectors and needs a Fortran compiler this image lacks).  It is pinned

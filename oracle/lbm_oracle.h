@@ -3,8 +3,9 @@
  *
  * The oracle is a plain C++ restatement of the geirev/LBM per-timestep path
  * (Fortran 90 / CUDA Fortran, built with nvfortran or gfortran).  It exists
- * so that tests, the smoke check and the CPU-baseline leg of the benchmark
- * can compare the CUDA library against the reference's arithmetic.  Nothing
+ * so that tests and the smoke check can compare the CUDA library against the
+ * reference's arithmetic, and so that the benchmark's CPU legs (the CPU
+ * baseline and the reference arm) can time it.  Nothing
  * in the product library links, loads or calls it.
  *
  * Parity status: UNPINNED against reference outputs.  The reference ships no

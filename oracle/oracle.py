@@ -1,7 +1,8 @@
 """ctypes wrapper of the CPU oracle (TEST INFRASTRUCTURE ONLY).
 
-Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this module; it is the checker, never the product.
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py``
+(the CPU baseline and the reference arm, ``--impl reference``) may import this
+module; it is the checker, never the product.
 
 Array conventions follow the reference's Fortran layout viewed from numpy in
 C order:

@@ -1,6 +1,6 @@
 """Fused state path (one kernel per step + boundary kernels) vs the oracle.
 
-Tolerance (north star): rho, u and f within a relative L2 of 1e-5 of the
+Tolerance (the target for this path): rho, u and f within a relative L2 of 1e-5 of the
 reference's FP32 arithmetic after 200 steps of the 128x64x64 sphere case.
 The oracle's own FP32-vs-FP64 drift on that case is 1.6e-6 (f, rho) and
 7.4e-6 (velocity vector); the single components v and w, which are small,
@@ -263,7 +263,7 @@ def test_sphere_200_steps_parity():
 
 def test_f16_storage_error_budget():
     """FP16-offset storage against the FP64 oracle on a small case: relative L2
-    of rho and u at most 1e-3 (the north-star bound after 1000 steps)."""
+    of rho and u at most 1e-3 (the bound the FP16 storage must keep after 1000 steps)."""
     wl = SMALL.with_(steps=60)
     blank = W.blanking(wl)
     turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
