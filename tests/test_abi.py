@@ -85,9 +85,25 @@ def test_params_struct_matches_header():
 
 
 def test_null_context_is_an_error_not_a_crash(lib):
-    assert lib.lbm_step(None, 1) == _lib.LBM_ERR_ARG
-    assert lib.lbm_destroy(None) == _lib.LBM_ERR_ARG
-    assert lib.lbm_postcoll(None, None, None, None, None, None, None, None) == _lib.LBM_ERR_ARG
+    """Every entry point that takes a context (or an ensemble) as its first
+    argument answers LBM_ERR_ARG to a null one, before touching the GPU."""
+    no_context = {"lbm_create", "lbm_abi_version", "lbm_last_error", "lbm_ensemble_last_error",
+                  "lbm_ensemble_create", "lbm_mass_momentum_noalloc"}
+    checked = 0
+    for name in header_functions():
+        if name in no_context:
+            continue
+        args = []
+        for t in _lib.SIGNATURES[name]:
+            if t is ctypes.c_void_p or not hasattr(t, "_type_") or isinstance(t._type_, type):
+                args.append(None)                       # pointers, the context first
+            elif t._type_ in "fd":
+                args.append(0.0)
+            else:
+                args.append(1)
+        assert getattr(lib, name)(*args) == _lib.LBM_ERR_ARG, name
+        checked += 1
+    assert checked >= 70
 
 
 def test_create_rejects_bad_params_before_touching_the_gpu(lib):
