@@ -177,3 +177,34 @@ def test_forcing_changes_momentum_by_minus_the_force(nl):
     g = f0.copy()
     o.forcings_apply(g, np.zeros_like(F), rho, u, v, w)
     assert np.array_equal(g, f0)
+
+
+def test_oracle_results_do_not_depend_on_the_thread_count():
+    """No oracle loop reduces across OpenMP threads, so the CPU baseline's thread
+    count changes its speed, never its numbers: 1 and 4 threads agree bit for bit
+    over a run with solids and the turbulence slice."""
+    import numpy as np
+    from lbm_b200 import workloads as W
+    from oracle import oracle as O
+    wl = W.Workload("threads", 20, 10, 8, 27, steps=4, sphere=(6, 5, 4, 2), lturb=True, ampl=1e-3, nrturb=3)
+    cfg = O.Config(wl.nx, wl.ny, wl.nz, 27, iturb_pos=5, lsolids=True, lturb=True, nrturb=wl.nrturb, ampl=wl.ampl)
+    blank = W.blanking(wl)
+    turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
+    import os
+    before = O._threads
+    outs = []
+    try:
+        for n in (1, 4):
+            O.set_threads(n)
+            o = O.Oracle(cfg, np.float32)
+            rho, u, v, w = W.initial_macro(wl)
+            uvel = W.inflow_profile(wl)
+            fA, fB = o.zeros_f(), o.zeros_f()
+            o.init(fA, fB, rho, u, v, w, uvel)
+            tau = np.full(cfg.sshape, 3 * np.float32(1e-4) + 0.5, np.float32)
+            o.run(fA, fB, rho, u, v, w, tau, uvel, wl.steps, blanking=blank, uu=turb[0], vv=turb[1], ww=turb[2])
+            outs.append((fA, fB, rho, u, v, w))
+    finally:
+        O.set_threads(before if before else (os.cpu_count() or 1))
+    for a, b in zip(*outs):
+        assert np.array_equal(a.view(np.int32), b.view(np.int32))
