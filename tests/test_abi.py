@@ -154,3 +154,49 @@ int main(void) {
     assert out.returncode == 0, out.stderr
     version, bad, null = (int(x) for x in out.stdout.split())
     assert version == lib.lbm_abi_version() and bad == _lib.LBM_ERR_ARG and null == 1
+
+
+def test_fortran_interfaces_match_the_c_signatures():
+    """Each bind(C) interface of include/lbm_b200_iface.F90 has the C function's
+    argument count, and each argument's declaration passes what the C side
+    expects: device and host addresses as type(c_ptr), value (or a Fortran
+    variable by reference where C takes int64_t* / double* / a struct),
+    integers as integer(c_int32_t / c_int64_t), value, reals as real(c_float /
+    c_double), value."""
+    src = open(os.path.join(ROOT, "include", "lbm_b200_iface.F90")).read()
+    src = re.sub(r"!.*", "", src)                                   # comments
+    src = re.sub(r"&\s*\n\s*&?", " ", src)                          # continuation lines
+    blocks = re.findall(r'function\s+(lbm_\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name="(lbm_\w+)"\)(.*?)end function',
+                        src, flags=re.S)
+
+    def fortran_kind(decl):
+        d = decl.replace(" ", "").lower()
+        for prefix, k in (("type(c_ptr),value", "ptr"), ("integer(c_int32_t),value", "i32"),
+                          ("integer(c_int),value", "i32"), ("integer(c_int64_t),value", "i64"),
+                          ("real(c_float),value", "f32"), ("real(c_double),value", "f64")):
+            if d.startswith(prefix):
+                return k
+        return "ref"                                                # passed by reference: a pointer in C
+
+    c_kind = {ctypes.c_void_p: ("ptr", "ref"), ctypes.c_int32: ("i32",), ctypes.c_int64: ("i64",),
+              ctypes.c_uint64: ("i64",), ctypes.c_float: ("f32",), ctypes.c_double: ("f64",)}
+    checked = 0
+    for _, args, cname, body in blocks:
+        if cname not in _lib.SIGNATURES:
+            continue
+        names = [a.strip().lower() for a in args.split(",") if a.strip()]
+        sig = _lib.SIGNATURES[cname]
+        assert len(names) == len(sig), (cname, names, len(sig))
+        kinds = {}
+        for line in body.splitlines():
+            if "::" in line:
+                decl, names_part = line.split("::", 1)
+                for v in names_part.split(","):
+                    v = v.strip().split("(")[0].strip().lower()
+                    if v:
+                        kinds[v] = fortran_kind(decl)
+        for a, t in zip(names, sig):
+            allowed = c_kind.get(t, ("ref",))
+            assert kinds.get(a) in allowed, (cname, a, kinds.get(a), allowed)
+        checked += 1
+    assert checked >= 75
