@@ -39,7 +39,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="turb_inflow_q27_512x256x256")
     ap.add_argument("--storage", choices=["f32", "f16"], default="f32")
-    ap.add_argument("--kernel", choices=["pull", "pair", "tma"], default=None,
+    ap.add_argument("--kernel", choices=["pull", "pair"], default=None,
                     help="steady step kernel (default: the library's choice)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

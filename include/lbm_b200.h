@@ -62,7 +62,6 @@ enum {
 
 /* steady step kernel of the fused state (lbm_set_kernel) */
 enum {
-    LBM_KERNEL_TMA = 0,    /* shared-memory tiles filled by bulk copies                      */
     LBM_KERNEL_PULL = 1,   /* direct coalesced global loads, one cell per thread              */
     LBM_KERNEL_PAIR = 2    /* (default) two cells per thread on the packed f32x2 pipes; needs
                               ihrr=1, even nx >= 4 (other cases run LBM_KERNEL_PULL)          */

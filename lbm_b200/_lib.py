@@ -25,7 +25,6 @@ LBM_STORE_F32 = 0
 LBM_STORE_F16 = 1
 LBM_STATUS_BAD_DENSITY = 1
 LBM_STATUS_TIMEOUT = 4
-LBM_KERNEL_TMA = 0
 LBM_KERNEL_PULL = 1
 LBM_KERNEL_PAIR = 2
 LBM_ENS_VARIANTS = 3

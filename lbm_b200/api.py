@@ -389,10 +389,9 @@ class Lbm:
         self._call("lbm_step_to", _ptr(dst))
 
     def set_kernel(self, which: str):
-        """Steady step kernel: "pair" (two cells per thread, default where it applies),
-        "pull" (one cell per thread) or "tma" (shared-memory tiles)."""
-        self._call("lbm_set_kernel", ctypes.c_int32({"tma": _lib.LBM_KERNEL_TMA, "pull": _lib.LBM_KERNEL_PULL,
-                                                          "pair": _lib.LBM_KERNEL_PAIR}[which]))
+        """Steady step kernel: "pair" (two cells per thread, default where it applies)
+        or "pull" (one cell per thread)."""
+        self._call("lbm_set_kernel", ctypes.c_int32({"pull": _lib.LBM_KERNEL_PULL, "pair": _lib.LBM_KERNEL_PAIR}[which]))
 
     def step_host(self, nsteps, uvel_host=None):
         """Steps with host buffers: uvel_host is a CPU float32 tensor (pinned for async copies)."""

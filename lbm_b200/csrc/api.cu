@@ -14,7 +14,6 @@
 #include "boundary.cuh"
 #include "ref_kernels.cuh"
 #include "state_kernels.cuh"
-#include "tma_step.cuh"
 #include "pair_step.cuh"
 
 using namespace lbm;
@@ -69,7 +68,6 @@ struct lbm_ctx {
     void* d_xg[2] = {nullptr, nullptr};  // compact x-ghost columns of each buffer (folded boundaries)
     bool idx32 = true;            // state small enough for 32-bit element offsets (k_step_fast)
     int kernel = LBM_KERNEL_PAIR; // steady step kernel (lbm_set_kernel); PULL where PAIR does not apply
-    int tma_grid[2] = {0, 0};     // persistent grid of k_step_tma per (wrap) variant, 0 = not sized yet
     int nsm = 148;
     int kopt_lo = 0, kopt_hi = 0;
     float* d_uvel = nullptr;      // uvel(nz)
@@ -418,27 +416,6 @@ StepArgs step_args(lbm_ctx* c) {
     return a;
 }
 
-// persistent grid of k_step_tma: resident CTAs per SM x SMs, at most one CTA per tile
-template <int Q, typename S, bool WRAP>
-int tma_launch(lbm_ctx* c, const S* src, S* dst, const StepArgs& a) {
-    const SoaGrid& g = c->sg;
-    const long long ntiles = (long long)((g.nx + kTileCells - 1) / kTileCells) * g.ny * g.nz;
-    const int smem = tma_smem_bytes<Q, S>();
-    int& grid = c->tma_grid[WRAP ? 1 : 0];
-    if (grid == 0) {
-        int occ = 0;
-        LBM_TRY(cuda_check(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_tma<Q, S, WRAP>, 128, smem),
-                           "occupancy"));
-        if (occ < 1) return fail(c, LBM_ERR_CUDA, "k_step_tma does not fit on an SM");
-        grid = occ * c->nsm;
-    }
-    const int nblk = (int)std::min<long long>(grid, ntiles);
-    k_step_tma<Q, S, WRAP><<<nblk, 128, smem, c->stream>>>(src, dst, a, ntiles);
-    c->launches++;
-    LBM_LAUNCHED(c, "fused step (tma)");
-    return LBM_OK;
-}
-
 template <int Q, typename S>
 void launch_gather_xg(lbm_ctx* c, int b) {
     const long long n = 2LL * Q * c->sg.ny * c->sg.nz;
@@ -485,8 +462,6 @@ int step_one(lbm_ctx* c) {
                 k_step_pair<Q, S, false, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
             c->launches++;
             LBM_LAUNCHED(c, "fused step (pair, j-slab tile)");
-        } else if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
-            LBM_TRY(tma_launch<Q, S, true>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
         } else if (pair_ok(c)) {
             if (c->force)
                 k_step_pair<Q, S, true, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
@@ -515,9 +490,7 @@ int step_one(lbm_ctx* c) {
     } else {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
-        if (c->idx32 && c->kernel == LBM_KERNEL_TMA) {
-            LBM_TRY(tma_launch<Q, S, false>(c, (const S*)c->buf[c->cur], (S*)c->buf[nxt], a));
-        } else if (pair_ok(c)) {
+        if (pair_ok(c)) {
             if (c->force)
                 k_step_pair<Q, S, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
             else
@@ -822,8 +795,7 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     chk(cudaGetDevice(&c->dev), "cudaGetDevice");
     if (rc == LBM_OK) chk(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev), "cudaDeviceGetAttribute");
     c->stream = nullptr;
-    // + 1 KiB: the bulk copies of k_step_tma read up to ~100 elements past the last row
-    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem + 1024;
+    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem;
     for (int b = 0; b < 2 && rc == LBM_OK; ++b) {
         chk(cudaMalloc(&c->own[b], nbuf), "cudaMalloc(state)");
         if (rc == LBM_OK) chk(cudaMemset(c->own[b], 0, nbuf), "cudaMemset(state)");
@@ -1457,7 +1429,7 @@ int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz
 
 int lbm_set_kernel(lbm_ctx* c, int32_t which) {
     if (!c) return LBM_ERR_ARG;
-    if (which != LBM_KERNEL_TMA && which != LBM_KERNEL_PULL && which != LBM_KERNEL_PAIR)
+    if (which != LBM_KERNEL_PULL && which != LBM_KERNEL_PAIR)
         return fail(c, LBM_ERR_ARG, "set_kernel: unknown kernel");
     c->kernel = which;
     return LBM_OK;

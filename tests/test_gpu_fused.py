@@ -140,23 +140,6 @@ def test_dp_build_run_matches_fp64_oracle(nl):
 
 @pytest.mark.parametrize("nl", [19, 27])
 @pytest.mark.parametrize("storage", ["f32", "f16"])
-def test_tma_kernel_matches_pull_kernel(nl, storage):
-    """The shared-memory-tile step kernel gives the pull kernel's results (round-off)."""
-    wl = SMALL.with_(nl=nl, nx=300)        # three tiles per row, the last one partial
-    blank = W.blanking(wl)
-    turb = W.turbulence_fields(wl.ny, wl.nz, wl.nrturb, 3)
-    a = run_gpu(wl, 12, 5, blank, turb, storage=storage, kernel="pull")
-    b = run_gpu(wl, 12, 5, blank, turb, storage=storage, kernel="tma")
-    e = errors(b, a)
-    assert all(v < 1e-6 for v in e.values()), e
-    if storage == "f32":
-        ref32 = run_oracle(wl, 12, np.float32, 5, blank, turb)
-        ref64 = run_oracle(wl, 12, np.float64, 5, blank, turb)
-        compare_to_floor(b, ref32, ref64, "tma")
-
-
-@pytest.mark.parametrize("nl", [19, 27])
-@pytest.mark.parametrize("storage", ["f32", "f16"])
 @pytest.mark.parametrize("iturb", [5, 6])
 @pytest.mark.parametrize("kernel", ["pair"])
 def test_pair_kernel_matches_oracle(nl, storage, iturb, kernel):
