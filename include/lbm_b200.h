@@ -115,13 +115,13 @@ int lbm_macrovars(lbm_ctx* ctx, float* rho, float* u, float* v, float* w, const 
 /* regularization(f,feq,u,v,w): f = R(f - feq)   m_regularization.F90:4 */
 int lbm_regularization(lbm_ctx* ctx, float* f, const float* feq, const float* u, const float* v, const float* w);
 
-/* vreman(f,tau): tau from non-equilibrium f     m_vreman.F90:187 */
+/* vreman(f,tau): tau from non-equilibrium f     m_vreman.F90:5 */
 int lbm_vreman(lbm_ctx* ctx, const float* f, float* tau);
 
 /* compute_fneq(f,feq): f = f - feq              m_compute_fneq.F90:4 */
 int lbm_compute_fneq(lbm_ctx* ctx, float* f, const float* feq);
 
-/* compute_f(f,feq): f = feq + f                 m_compute_f.F90:84 */
+/* compute_f(f,feq): f = feq + f                 m_compute_f.F90:4 */
 int lbm_compute_f(lbm_ctx* ctx, float* f, const float* feq);
 
 /* boundarycond(f1,f2,uvel,...)     m_boundarycond.F90:14 (tracer/pottemp are off this path) */
@@ -276,9 +276,13 @@ int lbm_conservation(lbm_ctx* ctx, double* out_host);
  * f: reference-layout device array f(nl,0:nx+1,0:ny+1,0:nz+1); out: 4 doubles
  * (mass, mx, my, mz) in device memory; stream: cudaStream_t (NULL = legacy default).
  * The first call on a device looks up the array's device address, so make that call
- * before any stream capture.  Every call reuses the same array, each block overwriting
- * its own partial before the final sum reads it: calls that may overlap on the GPU
- * (different streams, or different host threads) race and must be serialised. */
+ * before any stream capture; the address is kept for the life of the device's context,
+ * so a process that calls cudaDeviceReset cannot use this entry point afterwards.
+ * Every call reuses the same array, each block overwriting its own partial before the
+ * final sum reads it: calls that may overlap on the GPU (different streams, or
+ * different host threads) race and must be serialised.  LBM_ERR_CUDA reports a failed
+ * launch of this call (or a context already broken by earlier work); an error left
+ * pending by the caller's own earlier launches is neither reported nor cleared. */
 int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz, int32_t nl, double* out,
                               void* stream);
 

@@ -73,7 +73,7 @@ module lbm_b200_iface
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, f, feq, u, v, w
       end function
-      ! call vreman(f,tau)                                m_vreman.F90:187
+      ! call vreman(f,tau)                                m_vreman.F90:5
       integer(c_int) function lbm_vreman(ctx, f, tau) bind(C, name="lbm_vreman")
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, f, tau
@@ -83,7 +83,7 @@ module lbm_b200_iface
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, f, feq
       end function
-      ! call compute_f(f,feq)                             m_compute_f.F90:84
+      ! call compute_f(f,feq)                             m_compute_f.F90:4
       integer(c_int) function lbm_compute_f(ctx, f, feq) bind(C, name="lbm_compute_f")
          import :: c_ptr, c_int
          type(c_ptr), value :: ctx, f, feq

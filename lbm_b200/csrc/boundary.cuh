@@ -47,7 +47,7 @@ struct SoaAcc {
 };
 
 // Up to 9 (outgoing l, reflected m) pairs of one closed face, computed on the
-// host by the reference's first-match search (m_boundary_k_closed_kernel.F90:160-166).
+// host by the reference's first-match search (m_boundary_k_closed_kernel.F90:35-46).
 struct FacePairs {
     int n;
     int8_t l[9], m[9];
@@ -151,7 +151,7 @@ __global__ void k_corners(Acc f1, Acc f2, CornerSet cs) {
     f1.cp(cs.l[t], i, j, k, f1, cs.l[t], i - cs.cx[t], j - cs.cy[t], k - cs.cz[t]);
 }
 
-// Inflow at i=0 and zero-gradient outflow at i=nx+1, m_boundary_i_inflow_kernel.F90:161-231.
+// Inflow at i=0 and zero-gradient outflow at i=nx+1, m_boundary_i_inflow_kernel.F90:56-111.
 // fghost(l) = f(l,1,j,k) - 2 w_l rho0 (cx u cos + cy u sin) / cs2; directions with
 // cx > 0 take fghost of their opposite.  In offset storage w_l cancels, and
 // opposite directions share w_l, so the same update holds for f - w_l.

@@ -109,7 +109,7 @@ __device__ __forceinline__ R collide(R (&fp)[Q], const MomentsT<R>& m, R drho, R
 
     R tau = tau_in;
     if (cp.ivreman) {
-        // Vreman (2004) with alpha = a2 (see header); guards as m_postcoll_kernel.F90:270-299
+        // Vreman (2004) with alpha = a2 (see header); guards as m_postcoll_kernel.F90:204-233
         R amag = axx * axx + ayy * ayy + azz * azz + R(2.0) * (axy * axy + axz * axz + ayz * ayz);
         amag = real_max(amag, lat_tiny<R>());
         const R b11 = cp.eps + axx * axx + axy * axy + axz * axz;

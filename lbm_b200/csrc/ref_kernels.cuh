@@ -17,7 +17,7 @@
 namespace lbm {
 
 
-// Equilibrium offsets feq_l - w_l (m_fequil3_kernel.F90:112-167 in closed form).
+// Equilibrium offsets feq_l - w_l (m_fequil3_kernel.F90:58-113 in closed form).
 template <int Q, typename R>
 __device__ __forceinline__ void equilibrium(R (&fe)[Q], R drho, R rho, R ux, R uy, R uz, bool cubic) {
     const R usq = ux * ux + uy * uy + uz * uz;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(128) k_ref_postcoll(R* f, R* tau, const R* rho
 }
 
 // drift: f(l,i,j,k) = feq(l,i-cx,j-cy,k-cz) over interior cells; a thread per
-// (l,i) of a row, as m_drift_kernel.F90:62-84 flattens it.  The source of
+// (l,i) of a row, as m_drift_kernel.F90:33-42 flattens it.  The source of
 // element e = (i-1) Q + l of a row is e minus the direction's distance Q d_l,
 // d_l = cx + (nx+2) cy + (nx+2)(ny+2) cz, taken from shared memory (a constant
 // read would serialise over the different l of a warp).  Each thread keeps
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(256) k_ref_drift(R* __restrict__ f, const R* _
     }
 }
 
-// macrovars over the ghost-inclusive grid, summation order of m_macrovars_kernel.F90:175-187
+// macrovars over the ghost-inclusive grid, summation order of m_macrovars_kernel.F90:35-49
 template <int Q, typename R = float>
 __global__ void __launch_bounds__(128) k_ref_macrovars(R* rho, R* u, R* v, R* w, const R* f,
                                                        RefGrid g) {
@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(128) k_ref_regularization(R* f, const R* feq, 
 }
 
 // vreman: tau from a non-equilibrium f with the standalone guards
-// (alphamag and beta start at 1e-5, no ablvisc; m_vreman_kernel.F90:281-325)
+// (alphamag and beta start at 1e-5, no ablvisc; m_vreman_kernel.F90:47-91)
 template <int Q, typename R = float>
 __global__ void __launch_bounds__(128) k_ref_vreman(const R* f, R* tau, RefGrid g, CollideParamsT<R> cp) {
     __shared__ R sm[128 * Q];

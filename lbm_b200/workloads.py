@@ -114,7 +114,7 @@ def initial_macro(wl: Workload, dtype=np.float32):
     """rho, u, v, w with rho = 1 and u = (uin, 0, 0) + U(-noise, noise) per component.
 
     The ghost shell is zero, as the reference leaves it after inipert
-    (m_inipert.F90:151-160 writes only 1..n)."""
+    (m_inipert.F90:121-130 writes only 1..n)."""
     rng = np.random.default_rng(wl.seed)
     shape = (wl.nz + 2, wl.ny + 2, wl.nx + 2)
     rho = np.zeros(shape, dtype)
@@ -131,12 +131,12 @@ def initial_macro(wl: Workload, dtype=np.float32):
 
 
 def inflow_profile(wl: Workload, dtype=np.float32):
-    """uvel(k) = uini * uvel_shear(k) with uvel_shear = 1 (m_inflow.F90:190-205)."""
+    """uvel(k) = uini * uvel_shear(k) with uvel_shear = 1 (m_inflow.F90:24-41)."""
     return np.full(wl.nz, wl.uin, dtype)
 
 
 def sphere_mask(nx, ny, nz, ic, jc, kc, r):
-    """lblanking of m_sphere.F90:278-284: (i-ic)^2+(j-jc)^2+(k-kc)^2 < r^2, ghosts included."""
+    """lblanking of m_sphere.F90:15-21: (i-ic)^2+(j-jc)^2+(k-kc)^2 < r^2, ghosts included."""
     k, j, i = np.meshgrid(np.arange(nz + 2), np.arange(ny + 2), np.arange(nx + 2), indexing="ij")
     return (((i - ic) ** 2 + (j - jc) ** 2 + (k - kc) ** 2) < r * r).astype(np.int32)
 

@@ -337,7 +337,7 @@ void regularization(const orc_params* p, T* f, const T* feq, const T* u, const T
 // ---------------------------------------------------------------------------
 template <typename T>
 void vreman(const orc_params* p, const T* f, T* tau) {
-    if (p->ivreman != 1) return;   // m_vreman.F90:211-213
+    if (p->ivreman != 1) return;   // m_vreman.F90:29-31
     const Lattice<T> L(p->nl);
     const Dims d(p);
     const T kinevisc = T(p->kinevisc);
@@ -411,7 +411,7 @@ void bnd_i_periodic(const Dims& d, T* f) {
                 f[d.f(l, d.nx + 1, j, k)] = f[d.f(l, 1, j, k)];
             }
 }
-// m_boundary_j_periodic_kernel.F90:73-76
+// m_boundary_j_periodic_kernel.F90:30-33
 template <typename T>
 void bnd_j_periodic(const Dims& d, T* f) {
 #pragma omp parallel for collapse(2) schedule(static)
@@ -422,7 +422,7 @@ void bnd_j_periodic(const Dims& d, T* f) {
                 f[d.f(l, i, d.ny + 1, k)] = f[d.f(l, i, 1, k)];
             }
 }
-// m_boundary_k_periodic_kernel.F90:99-113
+// m_boundary_k_periodic_kernel.F90:13-27
 template <typename T>
 void bnd_k_periodic(const Dims& d, T* f) {
     long plane = d.nl * d.nxg * d.nyg;
@@ -454,7 +454,7 @@ void bnd_i_closed(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int ip
                 }
             }
 }
-// m_boundary_j_closed_kernel.F90:92-114
+// m_boundary_j_closed_kernel.F90:35-46
 template <typename T>
 void bnd_j_closed(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int jplane, int opt) {
     int jghost = 0;
@@ -473,7 +473,7 @@ void bnd_j_closed(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int jp
                 }
             }
 }
-// m_boundary_k_closed_kernel.F90:146-168
+// m_boundary_k_closed_kernel.F90:24-46
 template <typename T>
 void bnd_k_closed(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int kplane, int opt) {
     int kghost = 0;
@@ -537,7 +537,7 @@ void bnd_i_j_edges(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int o
                     f1[d.f(l, e.ig, e.jg, k)] = f1[d.f(l, e.ii, e.ji, k)];
     }
 }
-// m_boundary_i_k_edges.F90:174-299
+// m_boundary_i_k_edges.F90:3-152
 template <typename T>
 void bnd_i_k_edges(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int opt) {
     struct E { int ig, kg, sx, sz, ii, ki; };
@@ -558,7 +558,7 @@ void bnd_i_k_edges(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int o
                     f1[d.f(l, e.ig, j, e.kg)] = f1[d.f(l, e.ii, j, e.ki)];
     }
 }
-// m_boundary_closed_corners.F90:191-252
+// m_boundary_closed_corners.F90:3-101
 template <typename T>
 void bnd_closed_corners(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, int opt) {
     const int corner[8][3] = {{0, 0, 0}, {0, 0, d.nz + 1}, {0, d.ny + 1, 0}, {0, d.ny + 1, d.nz + 1},
@@ -581,7 +581,7 @@ void bnd_closed_corners(const Lattice<T>& L, const Dims& d, T* f1, const T* f2, 
     }
 }
 
-// m_boundary_i_inflow_kernel.F90:161-231 (taperj = taperk = 1, m_boundarycond.F90:334-335)
+// m_boundary_i_inflow_kernel.F90:56-111 (taperj = taperk = 1, m_boundarycond.F90:334-335)
 template <typename T>
 void bnd_i_inflow(const orc_params* p, const Lattice<T>& L, const Dims& d, T* f, const T* uvel) {
     const T pi = T(3.1415927410125732);
@@ -660,7 +660,7 @@ void solids(const orc_params* p, T* f, const int32_t* blanking) {
                     for (int l = 1; l + 1 < d.nl; l += 2) std::swap(f[d.f(l, i, j, k)], f[d.f(l + 1, i, j, k)]);
 }
 
-// fequil3_block_kernel arithmetic for one cell, m_fequil3_block_kernel.F90:240-283
+// fequil3_block_kernel arithmetic for one cell, m_fequil3_block_kernel.F90:62-107
 template <typename T>
 void feq_block_cell(const orc_params* p, const Lattice<T>& L, T rr, const T vel[3], T* out) {
     const T ratio = L.inv6cs6 / L.inv2cs4;

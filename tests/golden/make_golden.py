@@ -47,7 +47,7 @@ def opposite(c, v):
 
 # ---- per-cell algebra (arrays: scalars (...), vel (...,3), f (..., nl)) ------
 def feq_cells(lat, rho, vel, ibgk, rest_h3=False):
-    """fequil3_kernel (m_fequil3_kernel.F90:112-167); rest_h3 selects the
+    """fequil3_kernel (m_fequil3_kernel.F90:58-113); rest_h3 selects the
     fequil3_block_kernel variant that adds H3 for every l (:273-283)."""
     c, w, H2, H3 = lat
     A2 = 4.5 * rho[..., None, None] * vel[..., :, None] * vel[..., None, :]
@@ -63,7 +63,7 @@ def feq_cells(lat, rho, vel, ibgk, rest_h3=False):
 
 
 def regularize_cells(lat, fneq, vel):
-    """R(fneq) as in m_postcoll_kernel.F90:189-244 / m_regularization_kernel.F90:107-172."""
+    """R(fneq) as in m_postcoll_kernel.F90:189-244 / m_regularization_kernel.F90:44-114."""
     c, w, H2, H3 = lat
     a2 = np.einsum("lpq,...l->...pq", H2, fneq)
     a3 = (vel[..., :, None, None] * a2[..., None, :, :] + vel[..., None, :, None] * np.swapaxes(a2, -1, -2)[..., :, None, :]
@@ -72,7 +72,7 @@ def regularize_cells(lat, fneq, vel):
 
 
 def vreman_tau(lat, fneq, kinevisc, smag, ablk, standalone=False):
-    """Vreman nu_t: m_postcoll_kernel.F90:255-304 or m_vreman_kernel.F90:281-325."""
+    """Vreman nu_t: m_postcoll_kernel.F90:189-239 or m_vreman_kernel.F90:47-91."""
     c, w, H2, H3 = lat
     alpha = np.einsum("lpq,...l->...pq", H2, fneq)
     eps = np.sqrt(np.finfo(np.float64).tiny)
