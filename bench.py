@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-f16", action="store_true", help="skip the FP16-offset storage comparison")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP16 error leg (city workload, 1000 steps, against the FP64 build)")
+    ap.add_argument("--no-q19", action="store_true", help="skip the D3Q19 leg of the default workload")
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
     ap.add_argument("--adjoint", action="store_true",
@@ -151,7 +154,10 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (restatement of the reference's OpenMP CPU path)
+# CPU baseline: the oracle (restatement of the reference's OpenMP CPU path),
+# timed by oracle/cpu_baseline.py in a fresh process that loads neither torch
+# nor CUDA; both CPU legs (cpu_baseline and --impl reference) time the same
+# 512x256x32 slab of the workload with one oracle run(n) call
 # ---------------------------------------------------------------------------
 def cpu_threads():
     try:
@@ -160,60 +166,24 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def oracle_case(wl, nz_s):
-    import numpy as np
-    from lbm_b200 import workloads as W
-    from oracle import oracle as O
-    s = wl.with_(nz=nz_s)
-    cfg = O.Config(s.nx, s.ny, s.nz, s.nl, ibnd=s.ibnd, jbnd=s.jbnd, kbnd=s.kbnd, iturb_pos=10,
-                   lturb=s.lturb, nrturb=s.nrturb, ampl=s.ampl, kinevisc=s.kinevisc, smagorinsky=s.smagorinsky)
-    o = O.Oracle(cfg, np.float32)
-    rho, u, v, w = W.initial_macro(s)
-    uvel = W.inflow_profile(s)
-    fA, fB = o.zeros_f(), o.zeros_f()
-    o.init(fA, fB, rho, u, v, w, uvel)
-    tau = np.full(cfg.sshape, 3 * np.float32(s.kinevisc) + 0.5, np.float32)
-    kw = {}
-    if s.lturb:
-        uu, vv, ww = W.turbulence_fields(s.ny, s.nz, s.nrturb, s.seed)
-        kw = dict(uu=uu, vv=vv, ww=ww)
-    state = dict(fA=fA, fB=fB, rho=rho, u=u, v=v, w=w, tau=tau, uvel=uvel, kw=kw, it=0)
-
-    def run(n):
-        o.run(state["fA"], state["fB"], state["rho"], state["u"], state["v"], state["w"], state["tau"],
-              state["uvel"], n, it0=state["it"], **state["kw"])
-        state["it"] += n
-    return s, run
+def cpu_leg(wl, steps=None, warmup=2, budget_s=15.0):
+    import subprocess
+    cmd = [sys.executable, "-m", "oracle.cpu_baseline", "--workload", wl.name, "--warmup", str(warmup)]
+    cmd += ["--steps", str(steps)] if steps is not None else ["--budget-s", str(budget_s)]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, check=True)
+    return json.loads(out.stdout.strip().splitlines()[-1])
 
 
-def cpu_sample(wl, budget_s, steps_hint):
-    """Pick the thickest k-slab of the workload that runs steps_hint steps within budget_s."""
-    from oracle import oracle as O
-    O.set_threads(cpu_threads())
-    probe, run = oracle_case(wl, 4)
-    t0 = time.perf_counter()
-    run(1)
-    rate = probe.cells / (time.perf_counter() - t0)          # LUP/s
-    nz_s = int(budget_s * rate / (max(steps_hint, 1) * wl.nx * wl.ny))
-    return max(2, min(wl.nz, nz_s))
+def cpu_sample_text(r):
+    return ("%dx%dx%d k-slab of the %s workload (%s FP32, same physics), %d steps in one run() call, %.1f s; C++ "
+            "restatement of the reference's OpenMP CPU path (the Fortran reference has no compiler in this image), "
+            "%d OpenMP threads on %s, fresh process without torch/CUDA"
+            % (*r["slab"], r["workload"], r["lattice"], r["steps"], r["seconds"], r["threads"], r["cpu"]))
 
 
 def cpu_baseline(wl):
-    nz_s = cpu_sample(wl, 15.0, 3)
-    s, run = oracle_case(wl, nz_s)
-    run(1)
-    n = 0
-    t0 = time.perf_counter()
-    while True:
-        run(1)
-        n += 1
-        el = time.perf_counter() - t0
-        if el > 10.0 or n >= 50:
-            break
-    mlups = s.cells * n / el / 1e6
-    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": cpu_threads(), "kind": "port",
-            "sample": "%dx%dx%d D3Q%d FP32 slab of the workload (same physics), %d steps in %.1f s, OpenMP %d threads"
-                      % (s.nx, s.ny, s.nz, s.nl, n, el, cpu_threads())}
+    r = cpu_leg(wl)
+    return {"value": r["value"], "unit": "MLUPS", "cores": r["threads"], "kind": "port", "sample": cpu_sample_text(r)}
 
 
 # ---------------------------------------------------------------------------
@@ -223,23 +193,15 @@ def run_reference(a, wl):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    nz_s = cpu_sample(wl, 90.0, a.warmup + a.steps)
-    s, run = oracle_case(wl, nz_s)
-    if a.warmup > 0:
-        run(a.warmup)
-    t0 = time.perf_counter()
-    run(a.steps)
-    el = time.perf_counter() - t0
-    mlups = s.cells * a.steps / el / 1e6
-    sample = ("%dx%dx%d k-slab of the %s workload, D3Q%d FP32, same physics; C++ restatement of the reference's "
-              "OpenMP CPU path (the Fortran reference has no compiler in this image)" % (s.nx, s.ny, s.nz, wl.name, s.nl))
-    line = {"impl": "reference", "metric": METRIC, "value": round(mlups, 3), "unit": "MLUPS", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(el / max(a.steps, 1) * 1e3, 3),
+    r = cpu_leg(wl, steps=a.steps, warmup=a.warmup)
+    mlups = r["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": mlups, "unit": "MLUPS", "n_gpus": a.gpus,
+            "steps": r["steps"], "warmup": a.warmup, "ms_per_step": round(r["seconds"] / r["steps"] * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_of(wl, "f32", a.gpus),
-            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cpu_threads(), "kind": "port",
-                             "sample": sample},
-            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "cpu_baseline": {"value": mlups, "unit": "MLUPS", "cores": r["threads"], "kind": "port",
+                             "sample": cpu_sample_text(r)},
+            "e2e": {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -386,6 +348,29 @@ def rel_l2_pair(a, b):
     return {"rho": float(torch.linalg.vector_norm(ra - rb) / torch.linalg.vector_norm(rb)),
             "rho_minus_1": float(torch.linalg.vector_norm(ra - rb) / torch.linalg.vector_norm(rb - 1.0)),
             "u": float(torch.linalg.vector_norm(ua - ub) / torch.linalg.vector_norm(ub))}
+
+
+def accuracy_errors(big, steps):
+    """FP16-offset storage and plain FP32 (fused step, the library's default
+    kernels) on `big` after `steps` steps, against the same run in FP64 through
+    the DP build's per-call entry points on the GPU and against each other."""
+    import torch
+    t0 = time.perf_counter()
+    f32, s32 = gpu_run_macro(big, "f32", steps)
+    f16, s16 = gpu_run_macro(big, "f16", steps)
+    torch.cuda.empty_cache()
+    f64, s64 = dp_run_macro(big, steps)
+    torch.cuda.empty_cache()
+    e16, e32, e1632 = rel_l2_pair(f16, f64), rel_l2_pair(f32, f64), rel_l2_pair(f16, f32)
+    return {"rel_l2_rho_vs_fp64": e16["rho"], "rel_l2_rho_minus_1_vs_fp64": e16["rho_minus_1"],
+            "rel_l2_u_vs_fp64": e16["u"], "rel_l2_rho_vs_f32": e1632["rho"], "rel_l2_u_vs_f32": e1632["u"],
+            "f32_vs_fp64": {"rel_l2_rho": e32["rho"], "rel_l2_u": e32["u"]},
+            "error_bound": "relative L2 <= 1e-3 vs FP64",
+            "error_config": {"workload": big.name, "grid": [big.nx, big.ny, big.nz], "steps": steps,
+                             "solids": "%d seeded boxes, heights 10-40" % big.city,
+                             "fp64": "the DP build's per-call entry points (_f64) on the GPU, main.F90's init and step order",
+                             "u": "velocity vector field (u, v, w) over the interior cells"},
+            "error_status_flags": [s32, s16, s64], "error_leg_s": round(time.perf_counter() - t0, 1)}
 
 
 def accuracy_study(steps):
@@ -812,6 +797,32 @@ def slab_bench(a):
     return 0
 
 
+def lattice_leg(a, wl, hbm):
+    """The same timed run on another lattice of the workload (FP32 and FP16-offset storage)."""
+    import torch
+    out = {"workload": wl.name, "lattice": "D3Q%d" % wl.nl}
+    for storage in ("f32", "f16"):
+        s = make_solver(wl, storage, seed=wl.seed, kernel=a.kernel)
+        s.step(a.warmup)
+        ms, _, kms, kn = timed_steps(s, a.steps, None)
+        st = s.lbm.status()
+        s.close()
+        del s
+        torch.cuda.empty_cache()
+        k_ms = kms / max(kn, 1)
+        bl = bytes_per_lup(wl.nl, storage)
+        r = {"value": round(wl.cells * a.steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS",
+             "ms_per_step": round(ms / a.steps, 4), "kernel_ms": round(k_ms, 4), "bytes_per_lup": bl,
+             "roofline_frac": round(wl.cells * bl / (k_ms * 1e-3) / 1e9 / hbm, 4) if kn else None,
+             "status_flags": st}
+        if storage == "f32":
+            out.update(r)
+        else:
+            r["speedup_vs_f32"] = round(r["value"] / out["value"], 3)
+            out["f16_storage"] = r
+    return out
+
+
 def main():
     a = parse()
     if a.slabs and a.impl == "ours":
@@ -889,8 +900,14 @@ def main():
         ach16 = cells * bytes_per_lup(wl.nl, "f16") / (kms16 / max(kn16, 1) * 1e-3) / 1e9 if kn16 else None
         line["f16_storage"] = {"value": round(v16, 1), "unit": "MLUPS", "speedup_vs_f32": round(v16 / value, 3),
                                "roofline_frac": round(ach16 / hbm, 4) if ach16 else None,
-                               "kernel_ms": round(kms16 / max(kn16, 1), 4)}
+                               "kernel_ms": round(kms16 / max(kn16, 1), 4), "ms_per_step": round(ms16 / a.steps, 4)}
         torch.cuda.empty_cache()
+        if not a.no_accuracy and wl.name == W.CHANNEL_Q27.name:
+            # the stated-error half of the metric: the city workload after its 1000 steps
+            line["f16_storage"].update(accuracy_errors(W.CITY_Q27, W.CITY_Q27.steps))
+
+    if not a.no_q19 and world == 1 and wl.name == W.CHANNEL_Q27.name:
+        line["q19"] = lattice_leg(a, W.CHANNEL_Q19, hbm)
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)

@@ -283,7 +283,7 @@ void setup_boundaries(lbm_ctx* c) {
     c->fold = c->fold_cfg;
     c->kopt_lo = ko1;
     c->kopt_hi = koN;
-    // m_boundary_i_inflow_kernel.F90:191-193: cos(udir*pi/180), sin(udir*pi/180) in single precision
+    // m_boundary_i_inflow_kernel.F90:35,71-73: cos(udir*pi/180), sin(udir*pi/180) in single precision
     const float pi = 3.1415927410125732f;
     c->cosd = cosf(c->p.udir * pi / 180.0f);
     c->sind = sinf(c->p.udir * pi / 180.0f);
@@ -292,7 +292,7 @@ void setup_boundaries(lbm_ctx* c) {
 // Parameters of the FP64 entry points, as the reference's DP build (-r8) holds
 // them: every real in double precision, tiny() and eps = sqrt(tiny) of double
 // (m_postcoll.F90:46-47), pi the same literal as in single precision
-// (m_boundary_i_inflow_kernel.F90:191-193).
+// (m_boundary_i_inflow_kernel.F90:35,71-73).
 void set_params_f64(lbm_ctx* c, double kinevisc, double smagorinsky, double rho0, double udir) {
     c->cpd.kinevisc = kinevisc;
     c->cpd.cvre = 2.5 * smagorinsky * smagorinsky;
@@ -429,6 +429,20 @@ bool pair_shape_ok(const lbm_ctx* c) { return c->p.ihrr == 1 && c->p.nx % 2 == 0
 bool pair_ok(const lbm_ctx* c) { return c->kernel == LBM_KERNEL_PAIR && pair_shape_ok(c); }
 dim3 pair_grid(const lbm_ctx* c) { return dim3((unsigned)((c->p.nx / 2 + 127) / 128), c->p.ny, c->p.nz); }
 
+// the steady step from buffer cur into nxt, two cells per thread
+template <int Q, typename S, bool WRAP, bool FOLD>
+int pair_family_step(lbm_ctx* c, int nxt, const StepArgs& a) {
+    const S* src = (const S*)c->buf[c->cur];
+    S* dst = (S*)c->buf[nxt];
+    if (c->force)
+        k_step_pair<Q, S, WRAP, true, FOLD><<<pair_grid(c), 128, 0, c->stream>>>(src, dst, a);
+    else
+        k_step_pair<Q, S, WRAP, false, FOLD><<<pair_grid(c), 128, 0, c->stream>>>(src, dst, a);
+    c->launches++;
+    LBM_LAUNCHED(c, "fused step (pair)");
+    return LBM_OK;
+}
+
 template <int Q, typename S>
 int step_one(lbm_ctx* c) {
     if (c->force && !pair_ok(c))
@@ -456,19 +470,9 @@ int step_one(lbm_ctx* c) {
             if (!pair_ok(c))
                 return fail(c, LBM_ERR_UNSUPPORTED, "step: a j-slab tile in the folded configuration runs the "
                                                     "two-cells-per-thread kernel (LBM_KERNEL_PAIR, ihrr = 1, even nx >= 4)");
-            if (c->force)
-                k_step_pair<Q, S, false, true, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            else
-                k_step_pair<Q, S, false, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            c->launches++;
-            LBM_LAUNCHED(c, "fused step (pair, j-slab tile)");
+            LBM_TRY((pair_family_step<Q, S, false, true>(c, nxt, a)));
         } else if (pair_ok(c)) {
-            if (c->force)
-                k_step_pair<Q, S, true, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            else
-                k_step_pair<Q, S, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            c->launches++;
-            LBM_LAUNCHED(c, "fused step (pair)");
+            LBM_TRY((pair_family_step<Q, S, true, true>(c, nxt, a)));
         } else {
             if (c->idx32)
                 k_step_fast<Q, S, true><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
@@ -491,12 +495,7 @@ int step_one(lbm_ctx* c) {
         const int nxt = 1 - c->cur;
         LBM_TRY(prof_begin(c));
         if (pair_ok(c)) {
-            if (c->force)
-                k_step_pair<Q, S, false, true><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            else
-                k_step_pair<Q, S, false><<<pair_grid(c), 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
-            c->launches++;
-            LBM_LAUNCHED(c, "fused step (pair)");
+            LBM_TRY((pair_family_step<Q, S, false, false>(c, nxt, a)));
         } else {
             if (c->idx32)
                 k_step_fast<Q, S, false><<<grd, 128, 0, c->stream>>>((const S*)c->buf[c->cur], (S*)c->buf[nxt], a);
@@ -670,7 +669,7 @@ int regularization_run(lbm_ctx* c, R* f, const R* feq, const R* u, const R* v, c
 
 template <typename R>
 int vreman_run(lbm_ctx* c, const R* f, R* tau) {
-    if (c->p.ivreman != 1) return LBM_OK;   // m_vreman.F90:211-213
+    if (c->p.ivreman != 1) return LBM_OK;   // m_vreman.F90:29-31
     const CollideParamsT<R>& cp = cp_of<R>(c);
     if (c->p.nl == 27) k_ref_vreman<27, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, c->rg, cp);
     else k_ref_vreman<19, R><<<interior_rows(c), 128, 0, c->stream>>>(f, tau, c->rg, cp);
@@ -1392,7 +1391,9 @@ int lbm_conservation(lbm_ctx* c, double* out_host) {
 }
 
 // Device address of g_noalloc_partial on the current device, looked up once per
-// device (host code may not use the symbol itself as an address).
+// device (host code may not use the symbol itself as an address).  The cached
+// address belongs to the device's current context: a caller that resets the
+// device (cudaDeviceReset) cannot use this entry point afterwards.
 static int noalloc_scratch(double** out) {
     static std::mutex mu;
     static double* addr[128] = {nullptr};
@@ -1419,12 +1420,19 @@ int lbm_mass_momentum_noalloc(const float* f, int32_t nx, int32_t ny, int32_t nz
     double* scratch = nullptr;
     const int rc = noalloc_scratch(&scratch);
     if (rc != LBM_OK) return rc;
-    const RefGrid g{nx, ny, nz, nl};
+    RefGrid g{nx, ny, nz, nl};
     cudaStream_t s = (cudaStream_t)stream;
-    if (nl == 27) k_sum_ref<27><<<(int)nblocks, 256, 0, s>>>(f, g, scratch);
-    else k_sum_ref<19><<<(int)nblocks, 256, 0, s>>>(f, g, scratch);
-    k_sum_final<<<1, 256, 0, s>>>(scratch, (int)nblocks, out);
-    return cudaPeekAtLastError() == cudaSuccess ? LBM_OK : LBM_ERR_CUDA;
+    // cudaLaunchKernel returns this launch's own error, not an error left pending by
+    // the caller's earlier work (a sticky error of a broken context is reported, as
+    // by every CUDA call)
+    int nb = (int)nblocks;
+    void* sum_args[] = {(void*)&f, (void*)&g, (void*)&scratch};
+    const void* ksum = (nl == 27) ? (const void*)k_sum_ref<27> : (const void*)k_sum_ref<19>;
+    if (cudaLaunchKernel(ksum, dim3((unsigned)nb), dim3(256), sum_args, 0, s) != cudaSuccess) return LBM_ERR_CUDA;
+    void* fin_args[] = {(void*)&scratch, (void*)&nb, (void*)&out};
+    if (cudaLaunchKernel((const void*)k_sum_final, dim3(1), dim3(256), fin_args, 0, s) != cudaSuccess)
+        return LBM_ERR_CUDA;
+    return LBM_OK;
 }
 
 int lbm_set_kernel(lbm_ctx* c, int32_t which) {

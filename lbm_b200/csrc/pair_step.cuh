@@ -131,6 +131,40 @@ __device__ __forceinline__ float vreman_nut(float bb, float amag, const CollideP
     return (t > cp.eps) ? cp.cvre * sqrtf(t) : 0.0f;
 }
 
+// Reciprocal and square root by the approximate PTX instructions (rcp.approx,
+// sqrt.approx: one special-function instruction each, relative error a few
+// units in the last FP32 place).  The FP16-offset state keeps 11 significant
+// bits, so these errors vanish in its rounding, while the correctly rounded
+// forms cost a dozen instructions and a branch each; the FP32 state keeps the
+// correctly rounded forms.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+// 1/x of both cells: correctly rounded for FP32 storage, approximate for FP16
+template <typename S>
+__device__ __forceinline__ f2 rcp2(f2 x) {
+    if constexpr (sizeof(S) == 2) return make_float2(rcp_approx(x.x), rcp_approx(x.y));
+    else return make_float2(__frcp_rn(x.x), __frcp_rn(x.y));
+}
+// Vreman eddy viscosity of both cells from B_beta and |alpha|^2 (see vreman_nut)
+template <typename S>
+__device__ __forceinline__ f2 vreman_nut2(f2 bb, f2 sq, const CollideParams& cp) {
+    const float tiny = 1.17549435e-38f;
+    if constexpr (sizeof(S) == 2) {
+        const f2 t = mul2(bb, rcp2<S>(make_float2(fmaxf(sq.x, tiny), fmaxf(sq.y, tiny))));
+        return make_float2(t.x > cp.eps ? cp.cvre * sqrt_approx(t.x) : 0.0f, t.y > cp.eps ? cp.cvre * sqrt_approx(t.y) : 0.0f);
+    } else {
+        return make_float2(vreman_nut(bb.x, fmaxf(sq.x, tiny), cp), vreman_nut(bb.y, fmaxf(sq.y, tiny), cp));
+    }
+}
+
 // collide_rows() for two cells: fp receives the post-collision offsets times
 // store_scale<S>().  solid.x / solid.y flag the two cells.
 template <int Q, typename S>
@@ -161,11 +195,10 @@ __device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2
         f2 bb = sub2(mul2(b11, b22), mul2(b12, b12));
         bb = add2(bb, sub2(mul2(b11, b33), mul2(b13, b13)));
         bb = add2(bb, sub2(mul2(b22, b33), mul2(b23, b23)));
-        const f2 nut = make_float2(vreman_nut(bb.x, fmaxf(sq.x, 1.17549435e-38f), cp),
-                                   vreman_nut(bb.y, fmaxf(sq.y, 1.17549435e-38f), cp));
+        const f2 nut = vreman_nut2<S>(bb, sq, cp);
         tau = fma2(bc2(3.0f), add2(bc2(cp.kinevisc + abl), nut), bc2(0.5f));
     }
-    const f2 K = make_float2(1.0f - __frcp_rn(tau.x), 1.0f - __frcp_rn(tau.y));
+    const f2 K = sub2(bc2(1.0f), rcp2<S>(tau));
     const bool cubic = (cp.ibgk == 3);
     const f2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
     EmitConst2 k;
@@ -231,13 +264,13 @@ struct PairLoad<Q, S, Q> {
 
 __device__ __forceinline__ float comp(f2 v, int c) { return c ? v.y : v.x; }
 
-// Everything after the loads of one pair: moments, collision, turbulence slice,
-// solid swap, stores and the edge copy of the folded boundaries (FOLD).  (Variants
-// that moved the turbulence slice out of this kernel -- a one-cell post-pass, or a
-// captured FP32 copy finished by a second kernel -- measured slower on B200.)
-template <int Q, typename S, bool FOLD, bool FORCE = false>
-__device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, const StepArgs& a, long long o, int i,
-                                            int j, int k) {
+// Everything between the loads and the stores of one pair: moments, collision,
+// turbulence slice and external forcing, with the solid swap folded in.  On
+// return fp holds the post-collision offsets (times store_scale<S>()).  (Variants
+// that moved the turbulence slice out of the step kernel -- a one-cell post-pass,
+// or a captured FP32 copy finished by a second kernel -- measured slower on B200.)
+template <int Q, typename S, bool FORCE = false>
+__device__ __forceinline__ void pair_collide(f2 (&fp)[Q], const StepArgs& a, int i, int j, int k) {
     Moments2 m = moments_rows2<Q>(fp);
     if constexpr (sizeof(S) == 2) {
         const f2 is = bc2(1.0f / store_scale<S>());
@@ -247,10 +280,9 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
     }
     const f2 drho = m.s0;
     const f2 rho = add2(bc2(1.0f), m.s0);
-    const f2 inv = make_float2(__frcp_rn(rho.x), __frcp_rn(rho.y));
+    const f2 inv = rcp2<S>(rho);
     const f2 ux = mul2(m.jx, inv), uy = mul2(m.jy, inv), uz = mul2(m.jz, inv);
-    flag_bad_density(a.status, rho.x, ux.x, uy.x, uz.x);
-    flag_bad_density(a.status, rho.y, ux.y, uy.y, uz.y);
+    flag_bad_density2(a.status, rho, add2(add2(rho, ux), add2(uy, uz)));
     bool solid0 = false, solid1 = false;
     if (a.solid) {
         const unsigned short s2 =
@@ -304,14 +336,13 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
             fp[l + 1] = add2(fp[l + 1], sub2(dE, dO));
         }
     }
-    S* q = dst + o;
-#pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        char* qb = reinterpret_cast<char*>(q) + a.soffb[l];
-        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
-        else *reinterpret_cast<float2*>(qb) = fp[l];
-    }
-    if (FOLD && (i == 1 || i + 1 == a.g.nx)) {
+}
+
+// The edge copy of the folded boundaries: the post-collision populations of the
+// pair holding i = 1 or i = nx, into the compact edge array.
+template <int Q, typename S>
+__device__ __forceinline__ void pair_edge(const f2 (&fp)[Q], const StepArgs& a, int i, int j, int k) {
+    if (i == 1 || i + 1 == a.g.nx) {
         // the boundary kernel builds the inflow/outflow ghosts from these, read coalesced
         const long long nyz = (long long)a.g.ny * a.g.nz;
         const int c = (i == 1) ? 0 : 1;
@@ -322,6 +353,22 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
             else e[l * nyz] = comp(fp[l], c);
         }
     }
+}
+
+// Everything after the loads of one pair: pair_collide, the stores and the edge
+// copy of the folded boundaries (FOLD).
+template <int Q, typename S, bool FOLD, bool FORCE = false>
+__device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, const StepArgs& a, long long o, int i,
+                                            int j, int k) {
+    pair_collide<Q, S, FORCE>(fp, a, i, j, k);
+    S* q = dst + o;
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        char* qb = reinterpret_cast<char*>(q) + a.soffb[l];
+        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
+        else *reinterpret_cast<float2*>(qb) = fp[l];
+    }
+    if (FOLD) pair_edge<Q, S>(fp, a, i, j, k);
 }
 
 // One pair (i, i+1), i odd, of row (j, k): pull, collide, store.  WRAP: periodic

@@ -50,7 +50,7 @@ struct StepArgs {
     // folded boundaries
     int kopt_lo, kopt_hi;     // -1 no-slip, +1 free-slip at k=1 / k=nz
     const float* uvel;        // inflow profile uvel(nz)
-    float rho0, cosd, sind;   // inflow constants (m_boundary_i_inflow_kernel.F90:191-193)
+    float rho0, cosd, sind;   // inflow constants (m_boundary_i_inflow_kernel.F90:35,71-73)
     int* d_it_rw;             // step counter, advanced by the boundary kernel
     void* edge;               // post-collision populations at i=1 and i=nx: [side][l][k-1][j-1]
     int full_sector;          // x-ghost sectors hold nothing but the ghost and padding
@@ -66,6 +66,14 @@ struct StepArgs {
 __device__ __forceinline__ void flag_bad_density(int* status, float rho, float ux, float uy, float uz) {
     const float chk = rho + ux + uy + uz;
     const bool bad = !(rho > 0.0f) || !(fabsf(chk) < 1.0e30f);
+    const unsigned mask = __activemask();
+    const unsigned vote = __ballot_sync(mask, bad);
+    if (vote && (threadIdx.x & 31) == (__ffs(mask) - 1)) atomicOr(status, 1);
+}
+
+// flag_bad_density for two cells with one vote: rho of both cells and chk = rho + u + v + w of each
+__device__ __forceinline__ void flag_bad_density2(int* status, float2 rho, float2 chk) {
+    const bool bad = !(rho.x > 0.0f) || !(rho.y > 0.0f) || !(fabsf(chk.x) < 1.0e30f) || !(fabsf(chk.y) < 1.0e30f);
     const unsigned mask = __activemask();
     const unsigned vote = __ballot_sync(mask, bad);
     if (vote && (threadIdx.x & 31) == (__ffs(mask) - 1)) atomicOr(status, 1);
@@ -143,7 +151,7 @@ __device__ __forceinline__ void store_sector(S* p, S v, int slot) {
 //   * k-face threads, one per (i, j, face) with i in 1..nx: for each outgoing
 //     direction l of the face, f1(l,i,j,kg) = f1(l, i-cx, j-cy, kp) when the
 //     source is an interior cell, and f1(m,i,j,kg) = f2(l,i,j,kg) for the
-//     reflected direction m (m_boundary_k_closed_kernel.F90:157-168).
+//     reflected direction m (m_boundary_k_closed_kernel.F90:35-46).
 //   * x-ghost threads, one per (l, j, k): the inflow value of ghost (0,j,k)
 //     and the outflow value of ghost (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:
 //     184-231), written to the compact x-ghost array, and into the rows for
@@ -673,13 +681,30 @@ namespace lbm {
 
 // ---------------------------------------------------------------------------
 // FP64 conservation sums: mass sum(rho) and momentum sum(rho u) over the
-// interior cells.  Each cell's moments are formed in FP32 (as macrovars does)
-// and accumulated in FP64; blocks reduce with warp shuffles and write one
-// partial each, a single-block kernel adds the partials in a fixed order.
+// interior cells.  Every population is converted to FP64 once and each cell's
+// moments are formed and accumulated in FP64; blocks reduce with warp shuffles
+// and write one partial each, a single-block kernel adds the partials in a
+// fixed order.
 // ---------------------------------------------------------------------------
 struct Sum4 {
     double r, x, y, z;
 };
+
+// adds one cell's mass r0 + sum f_l and momentum sum c_l f_l to s, in FP64
+// (each population converted once; the FP32 offsets and populations are exact in FP64)
+template <int Q>
+__device__ __forceinline__ void cell_sum4(Sum4& s, const float (&v)[Q], double r0) {
+    double r = r0, x = 0.0, y = 0.0, z = 0.0;
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        const double d = (double)v[l];
+        r += d;
+        if (lat_cx(l) > 0) x += d; else if (lat_cx(l) < 0) x -= d;
+        if (lat_cy(l) > 0) y += d; else if (lat_cy(l) < 0) y -= d;
+        if (lat_cz(l) > 0) z += d; else if (lat_cz(l) < 0) z -= d;
+    }
+    s.r += r; s.x += x; s.y += y; s.z += z;
+}
 
 __device__ __forceinline__ Sum4 warp_sum4(Sum4 s) {
 #pragma unroll
@@ -718,16 +743,10 @@ __global__ void __launch_bounds__(256) k_sum_ref(const float* __restrict__ f, Re
         const int j = (int)((c / g.nx) % g.ny) + 1;
         const int k = (int)(c / ((long long)g.nx * g.ny)) + 1;
         const float* p = f + g.cell(i, j, k) * Q;
-        float r = 0.f, x = 0.f, y = 0.f, z = 0.f;
+        float v[Q];
 #pragma unroll
-        for (int l = 0; l < Q; ++l) {
-            const float v = p[l];
-            r += v;
-            macc(x, lat_cx(l), v);
-            macc(y, lat_cy(l), v);
-            macc(z, lat_cz(l), v);
-        }
-        s.r += r; s.x += x; s.y += y; s.z += z;
+        for (int l = 0; l < Q; ++l) v[l] = p[l];
+        cell_sum4<Q>(s, v, 0.0);
     }
     block_sum4_store(s, partial);
 }
@@ -743,9 +762,7 @@ __global__ void __launch_bounds__(256) k_sum_state(const S* __restrict__ src, So
         const int k = (int)(c / ((long long)g.nx * g.ny)) + 1;
         float fp[Q];
         PullMacro<Q, S, 0>::run(fp, src, g, g.off(i, j, k), j, wrap != 0);
-        const Moments m = moments<Q>(fp);
-        s.r += 1.0 + (double)m.s0;     // f = f' + w_l and sum w_l = 1
-        s.x += m.jx; s.y += m.jy; s.z += m.jz;
+        cell_sum4<Q>(s, fp, 1.0);     // f = f' + w_l and sum w_l = 1
     }
     block_sum4_store(s, partial);
 }
@@ -762,9 +779,7 @@ __global__ void __launch_bounds__(256) k_sum_stored(const S* __restrict__ src, S
         float fp[Q];
 #pragma unroll
         for (int l = 0; l < Q; ++l) fp[l] = Store<S>::to_f(src[(long long)l * g.dstride + g.off(i, j, k)]);
-        const Moments m = moments<Q>(fp);
-        s.r += 1.0 + (double)m.s0;
-        s.x += m.jx; s.y += m.jy; s.z += m.jz;
+        cell_sum4<Q>(s, fp, 1.0);
     }
     block_sum4_store(s, partial);
 }

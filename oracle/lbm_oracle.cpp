@@ -821,10 +821,10 @@ void run(const orc_params* p, T* fA, T* fB, T* rho, T* u, T* v, T* w, T* tau, co
         macrovars(p, rho, u, v, w, f1);
     }
     if (f1 != fA) {
-        long n = d.ncell() * d.nl;
-        std::vector<T> tmp(fA, fA + n);
-        std::memcpy(fA, fB, sizeof(T) * n);
-        std::memcpy(fB, tmp.data(), sizeof(T) * n);
+        // odd step count: exchange the contents in place (no temporary of the state's size)
+        const long n = d.ncell() * d.nl;
+#pragma omp parallel for schedule(static)
+        for (long e = 0; e < n; ++e) std::swap(fA[e], fB[e]);
     }
 }
 

@@ -65,12 +65,14 @@ def oracle_tiles(wl, ntiles, dtype, steps):
     return [(t["f1"], t["f2"], *t["R"]) for t in tiles]
 
 
-def gpu_tiles(wl, ntiles, steps, storage="f32"):
+def gpu_tiles(wl, ntiles, steps, storage="f32", kernel=None):
     from lbm_b200.slabs import SlabTile, step_local
     fA, fB, R, blank, uvel = global_start(wl)
     p = params_of(wl, iturb_pos=3, storage=storage)
     tiles = [SlabTile(p, r, ntiles) for r in range(ntiles)]
     for t in tiles:
+        if kernel is not None:
+            t.lbm.set_kernel(kernel)
         t.set_solids(cuda(blank.astype(np.int32)))
         t.set_inflow(cuda(uvel.astype(np.float32)))
         t.import_global(*(cuda(a.astype(np.float32)) for a in (fA, fB, *R)))
