@@ -49,6 +49,48 @@ def tile_slice(a, rank: int, ntiles: int):
     return a[:, j0 - 1:j0 + ny + 1]
 
 
+def plane_bytes(nx: int, nz: int, nl: int, storage: str = "f32") -> int:
+    """Bytes of one packed halo plane, as lbm_halo_plane_bytes reports them:
+    nl x (nz+2) x (nx+2) state values of 4 (FP32) or 2 (FP16) bytes."""
+    return nl * (nz + 2) * (nx + 2) * (2 if storage == "f16" else 4)
+
+
+def _weights(nl: int):
+    import numpy as np
+    c = np.array([[0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, -1, 1, 0, 0, -1, 1, 0, 0, -1, 1, -1, 1, 1, -1, -1, 1],
+                  [0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 1, -1, 0, 0, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1],
+                  [0, 0, 0, 0, 0, -1, 1, 0, 0, 0, 0, -1, 1, 1, -1, 1, -1, 1, -1, 1, -1, -1, 1, -1, 1, -1, 1]])[:, :nl]
+    s2 = (c * c).sum(0)
+    tab = {19: (1 / 3, 1 / 18, 1 / 36, 0.0), 27: (8 / 27, 2 / 27, 1 / 54, 1 / 216)}[nl]
+    return np.array([tab[k] for k in s2], dtype=np.float32)
+
+
+def plane_from_ref(f, j: int, storage: str = "f32"):
+    """Host mirror of lbm_halo_pack_j's plane layout: the bytes of plane j of a
+    reference-layout array f (nz+2, ny+2, nx+2, nl) as the state stores it,
+    values[l][k][i] (i = 0..nx+1 fastest) of the offset f - w_l, in FP32 or as
+    FP16 of (f - w_l) * 2^8."""
+    import numpy as np
+    nl = f.shape[-1]
+    off = (f[:, j].astype(np.float32) - _weights(nl)).transpose(2, 0, 1)      # (nl, nz+2, nx+2)
+    if storage == "f16":
+        return np.ascontiguousarray((off * np.float32(256.0)).astype(np.float16)).view(np.uint8).ravel()
+    return np.ascontiguousarray(off, dtype=np.float32).view(np.uint8).ravel()
+
+
+def plane_to_ref(buf, f, j: int, storage: str = "f32"):
+    """Inverse of plane_from_ref: write a packed plane into plane j of f."""
+    import numpy as np
+    nl = f.shape[-1]
+    nzp, nxp = f.shape[0], f.shape[2]
+    b = np.ascontiguousarray(buf, dtype=np.uint8)
+    if storage == "f16":
+        off = b.view(np.float16).astype(np.float32) / np.float32(256.0)
+    else:
+        off = b.view(np.float32)
+    f[:, j] = (off.reshape(nl, nzp, nxp).transpose(1, 2, 0) + _weights(nl)).astype(f.dtype)
+
+
 def exchange(send_south, send_north, recv_south, recv_north, south, north, group=None):
     """The halo exchange of one rank through torch.distributed: send_north goes
     to ``north`` and arrives there as its recv_south; send_south goes to

@@ -154,3 +154,24 @@ def test_halo_switch_refusals():
     with pytest.raises(LbmError, match="before the first import"):
         L.set_halo_j(True)
     L.close()
+
+
+@pytest.mark.parametrize("nl,storage", [(19, "f32"), (27, "f16")])
+def test_device_plane_layout_matches_the_host_mirror(nl, storage):
+    """lbm_halo_pack_j writes the bytes lbm_b200.slabs.plane_from_ref describes
+    (the layout the host-side exchange tests move between gloo ranks), and
+    lbm_halo_plane_bytes equals slabs.plane_bytes."""
+    from lbm_b200 import slabs
+    from lbm_b200.slabs import SlabTile
+    wl = W.Workload("slabs", 16, 12, 8, nl, steps=1, ibnd=1, jbnd=0, kbnd=12, noise=3e-3, sphere=(6, 5, 4, 2))
+    fA, fB, R, blank, uvel = global_start(wl)
+    t = SlabTile(params_of(wl, iturb_pos=3, storage=storage), 0, 2)
+    assert t.lbm.halo_plane_bytes() == slabs.plane_bytes(wl.nx, wl.nz, nl, storage)
+    f32 = [a.astype(np.float32) for a in (fA, fB, *R)]
+    t.import_global(*(cuda(a) for a in f32))
+    t.pack()
+    tile_f1 = np.ascontiguousarray(slabs.tile_slice(f32[0], 0, 2))
+    ny = wl.ny // 2
+    assert np.array_equal(host(t.send[0]), slabs.plane_from_ref(tile_f1, 1, storage))     # plane j = 1, to the south
+    assert np.array_equal(host(t.send[1]), slabs.plane_from_ref(tile_f1, ny, storage))    # plane j = ny, to the north
+    t.close()
