@@ -140,7 +140,7 @@ int lbm_boundarycond_adj(lbm_ctx* c, float* f1hat, float* f2hat, float* uvelhat)
 
 int lbm_state_bytes(lbm_ctx* c, int64_t* bytes) {
     if (!c || !bytes) return LBM_ERR_ARG;
-    *bytes = (int64_t)((size_t)c->p.nl * c->sg.dstride * c->elem + 1024);
+    *bytes = (int64_t)state_bytes_of(c);
     return LBM_OK;
 }
 
@@ -148,7 +148,7 @@ int lbm_state_copy(lbm_ctx* c, void* dst) {
     if (!c) return LBM_ERR_ARG;
     NEED(c, dst);
     if (c->state == ST_NONE) return fail(c, LBM_ERR_STATE, "state_copy: no state imported");
-    const size_t n = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    const size_t n = state_bytes_of(c);
     return cuda_check(c, cudaMemcpyAsync(dst, c->buf[c->cur], n, cudaMemcpyDeviceToDevice, c->stream), "state_copy");
 }
 

@@ -90,6 +90,9 @@ struct lbm_ctx {
 
 namespace {
 
+// bytes of one state buffer: nl direction blocks of dstride elements
+size_t state_bytes_of(const lbm_ctx* c) { return (size_t)c->p.nl * c->sg.dstride * c->elem; }
+
 int fail(lbm_ctx* c, int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
@@ -110,7 +113,9 @@ int cuda_check(lbm_ctx* c, cudaError_t e, const char* what) {
         int _rc = (__VA_ARGS__);        \
         if (_rc != LBM_OK) return _rc;  \
     } while (0)
-#define LBM_LAUNCHED(c, what) LBM_TRY(cuda_check((c), cudaPeekAtLastError(), (what)))
+// after a launch: the launch's error, which cudaGetLastError also clears (an error
+// left pending by earlier work of the calling thread is reported here and cleared too)
+#define LBM_LAUNCHED(c, what) LBM_TRY(cuda_check((c), cudaGetLastError(), (what)))
 
 // accumulate the elapsed time of recorded event pairs, then reuse them
 int prof_drain(lbm_ctx* c) {
@@ -794,7 +799,7 @@ int lbm_create(lbm_ctx** out, const lbm_params* p) {
     chk(cudaGetDevice(&c->dev), "cudaGetDevice");
     if (rc == LBM_OK) chk(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev), "cudaDeviceGetAttribute");
     c->stream = nullptr;
-    const size_t nbuf = (size_t)p->nl * c->sg.dstride * c->elem;
+    const size_t nbuf = state_bytes_of(c);
     for (int b = 0; b < 2 && rc == LBM_OK; ++b) {
         chk(cudaMalloc(&c->own[b], nbuf), "cudaMalloc(state)");
         if (rc == LBM_OK) chk(cudaMemset(c->own[b], 0, nbuf), "cudaMemset(state)");
@@ -1197,7 +1202,7 @@ static const int32_t kSnapMagic = 0x4c424d53;   // "LBMS"
 static SnapLayout snap_layout(const lbm_ctx* c) {
     auto up = [](size_t n) { return (n + 255) / 256 * 256; };
     SnapLayout L;
-    L.buf = up((size_t)c->p.nl * c->sg.dstride * c->elem + 1024);
+    L.buf = up(state_bytes_of(c));
     L.shell = up((size_t)c->p.nl * ghost_cells(c->sg) * c->elem);
     L.xg = c->fold ? up((size_t)2 * c->p.nl * c->p.ny * c->p.nz * c->elem) : 0;
     L.head = 256;
@@ -1232,7 +1237,7 @@ int lbm_state_snapshot(lbm_ctx* c, void* dst) {
     if (reinterpret_cast<uintptr_t>(dst) % 256 != 0) return fail(c, LBM_ERR_ARG, "state_snapshot: dst not 256-byte aligned");
     const SnapLayout L = snap_layout(c);
     char* d = static_cast<char*>(dst);
-    const size_t nbuf = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    const size_t nbuf = state_bytes_of(c);
     LBM_TRY(cuda_check(c, cudaMemcpyAsync(d, c->buf[c->cur], nbuf, cudaMemcpyDeviceToDevice, c->stream), "snapshot"));
     pack_ghosts(c, d + L.buf, c->buf[1 - c->cur], false);
     if (c->fold) {
@@ -1264,7 +1269,7 @@ int lbm_state_restore(lbm_ctx* c, const void* src) {
         return fail(c, LBM_ERR_ARG, "state_restore: not a snapshot of a context with these parameters");
     c->buf[0] = c->own[0];
     c->buf[1] = c->own[1];
-    const size_t nbuf = (size_t)c->p.nl * c->sg.dstride * c->elem + 1024;
+    const size_t nbuf = state_bytes_of(c);
     LBM_TRY(cuda_check(c, cudaMemcpyAsync(c->buf[0], s, nbuf, cudaMemcpyDeviceToDevice, c->stream), "restore"));
     pack_ghosts(c, const_cast<char*>(s) + L.buf, c->buf[1], true);
     if (c->fold) {

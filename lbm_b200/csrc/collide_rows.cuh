@@ -191,27 +191,46 @@ __device__ __forceinline__ float collide_rows(float (&fp)[Q], const Moments& m, 
 
 // Turbulence increment feq(rho, u+du) - feq(rho, u) added after the emission;
 // at a solid cell the increments are swapped with the populations they belong to.
+// Every operation rounds explicitly (the _rn intrinsics): plain a*b + c may be
+// fused differently in kernels compiled with different register budgets, and
+// the batched ensemble must reproduce the single-state kernels bit for bit.
+__device__ __forceinline__ float cdot_rn(int cx, int cy, int cz, float x, float y, float z) {
+    float r = 0.0f;
+    if (cx) r = cx > 0 ? __fadd_rn(r, x) : __fsub_rn(r, x);
+    if (cy) r = cy > 0 ? __fadd_rn(r, y) : __fsub_rn(r, y);
+    if (cz) r = cz > 0 ? __fadd_rn(r, z) : __fsub_rn(r, z);
+    return r;
+}
+
 template <int Q>
 __device__ __forceinline__ void add_turbulence(float (&fp)[Q], float rho, float ux, float uy, float uz,
                                                const TurbIn& tb, bool cubic, bool solid, float scale) {
-    const float usq = ux * ux + uy * uy + uz * uz;
-    const float dusq = tb.dux * (2.0f * ux + tb.dux) + tb.duy * (2.0f * uy + tb.duy) + tb.duz * (2.0f * uz + tb.duz);
-    const float usq2 = usq + dusq;
+    const float usq = __fmaf_rn(ux, ux, __fmaf_rn(uy, uy, __fmul_rn(uz, uz)));
+    const float dusq = __fmaf_rn(tb.dux, __fmaf_rn(2.0f, ux, tb.dux),
+                                 __fmaf_rn(tb.duy, __fmaf_rn(2.0f, uy, tb.duy), __fmul_rn(tb.duz, __fmaf_rn(2.0f, uz, tb.duz))));
+    const float usq2 = __fadd_rn(usq, dusq);
     const float sg = solid ? -1.0f : 1.0f;
-    fp[0] += lat_w<Q>(0) * scale * rho * (-1.5f * dusq);
+    fp[0] = __fmaf_rn(__fmul_rn(lat_w<Q>(0) * scale, rho), __fmul_rn(-1.5f, dusq), fp[0]);
 #pragma unroll
     for (int l = 1; l < Q; l += 2) {
         const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-        const float wr = lat_w<Q>(l) * scale * rho;
-        const float cu = cdot(cx, cy, cz, ux, uy, uz);
-        const float dcu = cdot(cx, cy, cz, tb.dux, tb.duy, tb.duz);
-        const float cun = cu + dcu;
-        const float dE = wr * (4.5f * dcu * (2.0f * cu + dcu) - 1.5f * dusq);
-        float od = 3.0f * dcu;
-        if (cubic) od += 4.5f * dcu * (cun * cun + cun * cu + cu * cu - usq2) - 4.5f * cu * dusq;
-        const float dO = sg * wr * od;
-        fp[l] += dE + dO;
-        fp[l + 1] += dE - dO;
+        const float wr = __fmul_rn(lat_w<Q>(l) * scale, rho);
+        const float cu = cdot_rn(cx, cy, cz, ux, uy, uz);
+        const float dcu = cdot_rn(cx, cy, cz, tb.dux, tb.duy, tb.duz);
+        const float cun = __fadd_rn(cu, dcu);
+        // 4.5 dcu (2 cu + dcu) - 1.5 dusq
+        const float e = __fmaf_rn(__fmul_rn(4.5f, dcu), __fmaf_rn(2.0f, cu, dcu), __fmul_rn(-1.5f, dusq));
+        const float dE = __fmul_rn(wr, e);
+        float od = __fmul_rn(3.0f, dcu);
+        if (cubic) {
+            // + 4.5 dcu (cun^2 + cun cu + cu^2 - usq2) - 4.5 cu dusq
+            const float poly = __fsub_rn(__fmaf_rn(cun, __fadd_rn(cun, cu), __fmul_rn(cu, cu)), usq2);
+            od = __fmaf_rn(__fmul_rn(4.5f, dcu), poly, od);
+            od = __fmaf_rn(__fmul_rn(-4.5f, cu), dusq, od);
+        }
+        const float dO = __fmul_rn(__fmul_rn(sg, wr), od);
+        fp[l] = __fadd_rn(fp[l], __fadd_rn(dE, dO));
+        fp[l + 1] = __fadd_rn(fp[l + 1], __fsub_rn(dE, dO));
     }
 }
 

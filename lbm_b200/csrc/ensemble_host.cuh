@@ -96,9 +96,9 @@ int ens_launch_step(lbm_ensemble* e, int parity) {
         case 128: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
         default: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
     }
-    LBM_TRY(echeck(e, cudaPeekAtLastError(), "ensemble step"));
+    LBM_TRY(echeck(e, cudaGetLastError(), "ensemble step"));
     k_ens_bc<Q, S><<<e->nblk[LBM_ENS_VARIANTS], 128, 0, e->stream>>>(ens_layout(e, LBM_ENS_VARIANTS), parity);
-    return echeck(e, cudaPeekAtLastError(), "ensemble boundaries");
+    return echeck(e, cudaGetLastError(), "ensemble boundaries");
 }
 
 int ens_launch(lbm_ensemble* e, int parity) {

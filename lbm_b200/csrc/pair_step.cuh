@@ -128,7 +128,7 @@ __device__ __forceinline__ void emit_row2(f2 (&fp)[Q], const EmitConst2& k) {
 
 __device__ __forceinline__ float vreman_nut(float bb, float amag, const CollideParams& cp) {
     const float t = bb / amag;
-    return (t > cp.eps) ? cp.cvre * sqrtf(t) : 0.0f;
+    return (t > cp.eps) ? __fmul_rn(cp.cvre, sqrtf(t)) : 0.0f;
 }
 
 // Reciprocal and square root by the approximate PTX instructions (rcp.approx,
@@ -159,19 +159,31 @@ __device__ __forceinline__ f2 vreman_nut2(f2 bb, f2 sq, const CollideParams& cp)
     const float tiny = 1.17549435e-38f;
     if constexpr (sizeof(S) == 2) {
         const f2 t = mul2(bb, rcp2<S>(make_float2(fmaxf(sq.x, tiny), fmaxf(sq.y, tiny))));
-        return make_float2(t.x > cp.eps ? cp.cvre * sqrt_approx(t.x) : 0.0f, t.y > cp.eps ? cp.cvre * sqrt_approx(t.y) : 0.0f);
+        return make_float2(t.x > cp.eps ? __fmul_rn(cp.cvre, sqrt_approx(t.x)) : 0.0f,
+                           t.y > cp.eps ? __fmul_rn(cp.cvre, sqrt_approx(t.y)) : 0.0f);
     } else {
         return make_float2(vreman_nut(bb.x, fmaxf(sq.x, tiny), cp), vreman_nut(bb.y, fmaxf(sq.y, tiny), cp));
     }
 }
 
-// collide_rows() for two cells: fp receives the post-collision offsets times
-// store_scale<S>().  solid.x / solid.y flag the two cells.
-template <int Q, typename S>
-__device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2 drho, f2 rho, f2 ux, f2 uy, f2 uz,
-                                              const CollideParams& cp, float abl, bool solid0, bool solid1) {
+// The collision state of two cells: the non-equilibrium moments a (a2 of the
+// regularized collision, Pi - I S0/3 - rho u u) and, through the Vreman eddy
+// viscosity, the relaxation factor K = 1 - 1/tau.
+struct CollideState2 {
+    f2 rho, drho, ux, uy, uz;
+    f2 rux, ruy, ruz;                 // rho u
+    f2 axx, ayy, azz, axy, axz, ayz, tr;
+    f2 K;
+};
+
+template <typename S>
+__device__ __forceinline__ CollideState2 collide_pre2(const Moments2& m, f2 drho, f2 rho, f2 ux, f2 uy, f2 uz,
+                                                      const CollideParams& cp, float abl) {
+    CollideState2 c;
+    c.rho = rho; c.drho = drho; c.ux = ux; c.uy = uy; c.uz = uz;
     const f2 third = bc2(1.0f / 3.0f);
     const f2 rux = mul2(rho, ux), ruy = mul2(rho, uy), ruz = mul2(rho, uz);
+    c.rux = rux; c.ruy = ruy; c.ruz = ruz;
     const f2 s3 = mul2(m.s0, third);
     const f2 axx = sub2(sub2(m.pxx, s3), mul2(rux, ux));
     const f2 ayy = sub2(sub2(m.pyy, s3), mul2(ruy, uy));
@@ -179,7 +191,8 @@ __device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2
     const f2 axy = sub2(m.pxy, mul2(rux, uy));
     const f2 axz = sub2(m.pxz, mul2(rux, uz));
     const f2 ayz = sub2(m.pyz, mul2(ruy, uz));
-    const f2 tr = add2(add2(axx, ayy), azz);
+    c.axx = axx; c.ayy = ayy; c.azz = azz; c.axy = axy; c.axz = axz; c.ayz = ayz;
+    c.tr = add2(add2(axx, ayy), azz);
     f2 tau = bc2(cp.tau0);
     if (cp.ivreman) {
         const f2 xx = mul2(axx, axx), yy = mul2(ayy, ayy), zz = mul2(azz, azz);
@@ -198,7 +211,17 @@ __device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2
         const f2 nut = vreman_nut2<S>(bb, sq, cp);
         tau = fma2(bc2(3.0f), add2(bc2(cp.kinevisc + abl), nut), bc2(0.5f));
     }
-    const f2 K = sub2(bc2(1.0f), rcp2<S>(tau));
+    c.K = sub2(bc2(1.0f), rcp2<S>(tau));
+    return c;
+}
+
+// collide_rows() for two cells: fp receives the post-collision offsets times
+// store_scale<S>().  solid.x / solid.y flag the two cells.
+template <int Q, typename S>
+__device__ __forceinline__ void collide_rows2(f2 (&fp)[Q], const Moments2& m, f2 drho, f2 rho, f2 ux, f2 uy, f2 uz,
+                                              const CollideParams& cp, float abl, bool solid0, bool solid1) {
+    const CollideState2 c = collide_pre2<S>(m, drho, rho, ux, uy, uz, cp, abl);
+    const f2 axx = c.axx, ayy = c.ayy, azz = c.azz, axy = c.axy, axz = c.axz, ayz = c.ayz, tr = c.tr, K = c.K;
     const bool cubic = (cp.ibgk == 3);
     const f2 usq = fma2(ux, ux, fma2(uy, uy, mul2(uz, uz)));
     EmitConst2 k;
@@ -263,6 +286,18 @@ struct PairLoad<Q, S, Q> {
 };
 
 __device__ __forceinline__ float comp(f2 v, int c) { return c ? v.y : v.x; }
+}  // namespace lbm
+
+#include "sep_emit.cuh"
+
+namespace lbm {
+// sep_transform27's values into the pair's population array
+template <int Q>
+struct SepArraySink {
+    f2 (&fp)[Q];
+    template <int L>
+    __device__ __forceinline__ void put(f2 v) { fp[L] = v; }
+};
 
 // Everything between the loads and the stores of one pair: moments, collision,
 // turbulence slice and external forcing, with the solid swap folded in.  On
@@ -291,6 +326,24 @@ __device__ __forceinline__ void pair_collide(f2 (&fp)[Q], const StepArgs& a, int
         solid1 = (s2 >> 8) != 0;
     }
     const float abl = a.abl ? a.abl[k - 1] : 0.0f;
+#ifndef LBM_NO_SEP
+    if constexpr (Q == 27 && sizeof(S) == 2) {
+        // FP16-offset D3Q27: the separable transform of sep_emit.cuh, the turbulence
+        // increment folded into its coefficients
+        const CollideState2 c = collide_pre2<S>(m, drho, rho, ux, uy, uz, a.cp, abl);
+        const bool cubic = a.cp.ibgk == 3;
+        SepCoef t = sep_coefficients<S>(c, make_float2(solid0 ? -1.0f : 1.0f, solid1 ? -1.0f : 1.0f), cubic);
+        if (a.uu != nullptr && (i == a.iturb || i + 1 == a.iturb)) {
+            const int cc = a.iturb - i;
+            const TurbIn tb = turb_at(a, a.iturb, j, k);
+            sep_add_turbulence<S>(t, cc, comp(rho, cc), comp(ux, cc), comp(uy, cc), comp(uz, cc), tb, cubic,
+                                  cc ? solid1 : solid0);
+        }
+        SepArraySink<Q> sink{fp};
+        sep_transform27(t, sink);
+    } else
+#endif
+    {
     collide_rows2<Q, S>(fp, m, drho, rho, ux, uy, uz, a.cp, abl, solid0, solid1);
     if (a.uu != nullptr && (i == a.iturb || i + 1 == a.iturb)) {
         const int c = a.iturb - i;
@@ -305,6 +358,7 @@ __device__ __forceinline__ void pair_collide(f2 (&fp)[Q], const StepArgs& a, int
             if (c) fp[l].y = t[l];
             else fp[l].x = t[l];
         }
+    }
     }
     if constexpr (FORCE) {
         // forcings_apply (m_forcings_apply_kernel.F90:47-213): f += feq2(rho, u - F/rho) - feq2(rho, u)
@@ -393,10 +447,18 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 #ifndef LBM_PAIR_MIN_BLOCKS
 #define LBM_PAIR_MIN_BLOCKS 5
 #endif
+// FP16-offset state: lower register caps (more resident warps) without spills;
+// measured best at 512x256x256: 8 blocks (64 registers) for D3Q27, 7 for D3Q19
+#ifndef LBM_PAIR_MIN_BLOCKS16_27
+#define LBM_PAIR_MIN_BLOCKS16_27 8
+#endif
+#ifndef LBM_PAIR_MIN_BLOCKS16_19
+#define LBM_PAIR_MIN_BLOCKS16_19 7
+#endif
 // Grid: x covers nx/2 pairs in blocks of 128 threads, y = j, z = k.  Needs
 // ihrr = 1 and nx even; offsets are 64-bit, so any state size.
 template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
-__global__ void __launch_bounds__(128, LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
+__global__ void __launch_bounds__(128, sizeof(S) == 2 ? (Q == 27 ? LBM_PAIR_MIN_BLOCKS16_27 : LBM_PAIR_MIN_BLOCKS16_19) : LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
                                                                         StepArgs a) {
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     if (i > a.g.nx) return;

@@ -88,9 +88,9 @@ __device__ __forceinline__ TurbIn turb_at(const StepArgs& a, int i, int j, int k
         if (lit == 0) lit = a.nrturb;
         const long long t = (long long)(j - 1) + (long long)a.g.ny * ((long long)(k - 1) + (long long)a.g.nz * lit);
         tb.on = true;
-        tb.dux = a.ampl * a.uu[t];
-        tb.duy = a.ampl * a.vv[t];
-        tb.duz = a.ampl * a.ww[t];
+        tb.dux = __fmul_rn(a.ampl, a.uu[t]);   // rounded here: never fused into a later add
+        tb.duy = __fmul_rn(a.ampl, a.vv[t]);
+        tb.duz = __fmul_rn(a.ampl, a.ww[t]);
     }
     return tb;
 }

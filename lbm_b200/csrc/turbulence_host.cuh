@@ -66,14 +66,14 @@ int lbm_inflow_turbulence_compute(lbm_ctx* c, float* uu, float* vv, float* ww, f
     if (rc == LBM_OK) {
         k_turb_spectrum<<<(unsigned)((nx_c + 255) / 256), 256, 0, c->stream>>>(X, s);
         c->launches++;
-        chk(cudaPeekAtLastError(), "turbulence spectrum");
+        chk(cudaGetLastError(), "turbulence spectrum");
     }
     if (rc == LBM_OK && cufftExecC2R(plan, reinterpret_cast<cufftComplex*>(X), Y) != CUFFT_SUCCESS)
         rc = fail(c, LBM_ERR_CUDA, "inflow_turbulence_compute: cufftExecC2R failed");
     if (rc == LBM_OK) {
         k_turb_ar1<1024><<<nf, 1024, 0, c->stream>>>(Y, outs, ny, nz, n1, n2, nrturb);
         c->launches++;
-        chk(cudaPeekAtLastError(), "turbulence levels");
+        chk(cudaGetLastError(), "turbulence levels");
     }
     // the temporaries are released after the work that uses them
     if (X || Y || outs) chk(cudaStreamSynchronize(c->stream), "inflow_turbulence_compute");
