@@ -428,6 +428,27 @@ void launch_gather_xg(lbm_ctx* c, int b) {
     c->launches++;
 }
 
+// A kernel launch that may begin while the previous kernel in the stream finishes
+// (programmatic dependent launch; the kernel waits for it, see pdl_enter).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+#ifdef LBM_NO_PDL
+    cfg.numAttrs = 0;
+#else
+    cfg.numAttrs = 1;
+#endif
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // the two-cells-per-thread kernel (pair_step.cuh) covers the regularized collision on even nx, at any
 // state size (64-bit byte offsets)
 bool pair_shape_ok(const lbm_ctx* c) { return c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
@@ -440,9 +461,11 @@ int pair_family_step(lbm_ctx* c, int nxt, const StepArgs& a) {
     const S* src = (const S*)c->buf[c->cur];
     S* dst = (S*)c->buf[nxt];
     if (c->force)
-        k_step_pair<Q, S, WRAP, true, FOLD><<<pair_grid(c), 128, 0, c->stream>>>(src, dst, a);
+        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, true, FOLD>, pair_grid(c), dim3(128), c->stream, src, dst, a),
+                           "fused step (pair)"));
     else
-        k_step_pair<Q, S, WRAP, false, FOLD><<<pair_grid(c), 128, 0, c->stream>>>(src, dst, a);
+        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, false, FOLD>, pair_grid(c), dim3(128), c->stream, src, dst,
+                                         a), "fused step (pair)"));
     c->launches++;
     LBM_LAUNCHED(c, "fused step (pair)");
     return LBM_OK;
@@ -487,10 +510,10 @@ int step_one(lbm_ctx* c) {
             LBM_LAUNCHED(c, "fused step");
         }
         LBM_TRY(prof_end(c));
-        const int nface = 2 * g.ny * ((g.nx + 127) / 128);
-        const long long nxg = (long long)Q * g.ny * g.nz;
-        const int nblk = nface + (int)((nxg + 127) / 128);
-        k_bc_fold<Q, S><<<nblk, 128, 0, c->stream>>>((S*)c->buf[nxt], (const S*)c->buf[c->cur], a, nface);
+        const int nface = bc_fold_face_blocks(g);
+        const int nblk = nface + (int)bc_fold_xg_blocks(g, Q);
+        LBM_TRY(cuda_check(c, launch_pdl(k_bc_fold<Q, S>, dim3(nblk), dim3(128), c->stream, (S*)c->buf[nxt],
+                                         (const S*)c->buf[c->cur], a, nface), "folded boundaries"));
         c->launches++;
         LBM_LAUNCHED(c, "folded boundaries");
         c->cur = nxt;

@@ -81,7 +81,7 @@ int ens_upload(lbm_ensemble* e) {
         c->cur = keep;
         d.buf[0] = c->buf[0];
         d.buf[1] = c->buf[1];
-        d.nface_blocks = 2 * c->sg.ny * ((c->sg.nx + 127) / 128);
+        d.nface_blocks = bc_fold_face_blocks(c->sg);
     }
     return echeck(e, cudaMemcpyAsync(e->d_mem, e->h_mem.data(), e->h_mem.size() * sizeof(EnsMember),
                                      cudaMemcpyHostToDevice, e->stream), "ensemble descriptors");
@@ -234,7 +234,7 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
                     nb = (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
-                    nb = 2LL * g.ny * ((g.nx + 127) / 128) + ((long long)e->nl * g.ny * g.nz + 127) / 128;
+                    nb = bc_fold_face_blocks(g) + bc_fold_xg_blocks(g, e->nl);
                 }
                 for (long long b = 0; b < nb; ++b) blk.push_back(make_int2((int)k, (int)b));
             }

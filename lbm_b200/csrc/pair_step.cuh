@@ -460,6 +460,7 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
 __global__ void __launch_bounds__(128, sizeof(S) == 2 ? (Q == 27 ? LBM_PAIR_MIN_BLOCKS16_27 : LBM_PAIR_MIN_BLOCKS16_19) : LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
                                                                         StepArgs a) {
+    pdl_enter();
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     if (i > a.g.nx) return;
     pair_cell<Q, S, WRAP, FORCE, FOLD>(src, dst, a, i, blockIdx.y + 1, blockIdx.z + 1);

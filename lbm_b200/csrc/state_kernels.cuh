@@ -187,14 +187,16 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
         }
         return;
     }
-    // x-ghost threads
-    const long long e = (long long)(vb - nface_blocks) * 128 + threadIdx.x;
+    // x-ghost threads: blocks of 128 j, then the direction l, then k (32-bit decode of the block index)
+    const int vbx = vb - nface_blocks;
+    const int nbj = (g.ny + 127) / 128;
+    const int rest = vbx / nbj;
+    const int j = (vbx - rest * nbj) * 128 + threadIdx.x + 1;
+    const int l = rest % Q;
+    const int k = rest / Q + 1;
+    if (vbx == 0 && threadIdx.x == 0) *a.d_it_rw += 1;   // the step counter advances once per step
+    if (j > g.ny || k > g.nz) return;
     const long long nyz = (long long)g.ny * g.nz;
-    if (e >= (long long)Q * nyz) return;
-    if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
-    const int j = (int)(e % g.ny) + 1;
-    const int l = (int)((e / g.ny) % Q);
-    const int k = (int)(e / ((long long)g.ny * Q)) + 1;
     const int cx = c_cx[l], cy = c_cy[l], cz = c_cz[l];
     S* fl = f1 + (long long)l * g.dstride;
     if (k == 1 || k == g.nz) {
@@ -236,8 +238,25 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
     }
 }
 
+// blocks of bc_fold_block: the k-face blocks, then the x-ghost blocks
+__host__ __device__ inline int bc_fold_face_blocks(const SoaGrid& g) { return 2 * g.ny * ((g.nx + 127) / 128); }
+__host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q) {
+    return (long long)((g.ny + 127) / 128) * Q * g.nz;
+}
+
+// Programmatic dependent launch (PDL) between the steady step kernel and the
+// boundary kernel: each kernel lets the next one in the stream be scheduled as
+// soon as all its own blocks have started, and every thread of the next one
+// waits at its start until the previous grid has completed and its memory is
+// visible.  Launched without the PDL attribute, both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
+    pdl_enter();
     bc_fold_block<Q, S>(f1, f2, a, nface_blocks, blockIdx.x);
 }
 
