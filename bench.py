@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-q19", action="store_true", help="skip the D3Q19 leg of the default workload")
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
+    ap.add_argument("--members", type=int, default=64,
+                    help="--ensemble: the first N of the 64 members (smaller captures for a profiler)")
     ap.add_argument("--adjoint", action="store_true",
                     help="checkpointed adjoint sweep of a probe-misfit loss (D3Q19 256x128x128 sphere, 100 steps)")
     ap.add_argument("--slabs", action="store_true",
@@ -416,7 +418,7 @@ def ensemble_bench(a):
         dist = replicas.init("nccl", timeout_s=300, device=torch.device("cuda", local))
     else:
         torch.cuda.set_device(0)
-    allm = W.ensemble_members()
+    allm = W.ensemble_members()[:a.members]
     mine = [m for k, m in enumerate(allm) if k % world == rank]
     ens = build_ensemble(mine, "f32")
     ens.step(1)
