@@ -47,6 +47,7 @@ def parse():
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP16 error leg (city workload, 1000 steps, against the FP64 build)")
     ap.add_argument("--no-q19", action="store_true", help="skip the D3Q19 leg of the default workload")
+    ap.add_argument("--no-ens", action="store_true", help="skip the batched-ensemble leg of the default run")
     ap.add_argument("--ensemble", action="store_true",
                     help="batched ensemble of 64 uneven D3Q19 members instead of the single-domain run")
     ap.add_argument("--members", type=int, default=64,
@@ -402,25 +403,16 @@ def accuracy_study(steps):
 # ---------------------------------------------------------------------------
 # batched ensemble (64 uneven D3Q19 members)
 # ---------------------------------------------------------------------------
-def ensemble_bench(a):
-    """Aggregate MLUPS of the batched ensemble (two launches per step for all
-    members, CUDA-graph replay, autotuned launch shape) against the same members
-    run one after another through the single-state path.  Under torchrun the
-    members are dealt out round-robin to the ranks (independent replicas)."""
+def ensemble_measure(a, members, dist=None):
+    """The batched ensemble of `members` (two launches per step for all members,
+    CUDA-graph replay, autotuned launch shape) against the same members run one
+    after another through the single-state path; the step kernel timed launch
+    by launch (lbm_ensemble_profile) for its roofline fraction."""
     import torch
-    from lbm_b200 import replicas, workloads as W
+    from lbm_b200 import replicas
     from lbm_b200 import _lib
     from lbm_b200.ensemble import build_ensemble
-    rank, local, world = replicas.env_rank()
-    dist = None
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist = replicas.init("nccl", timeout_s=300, device=torch.device("cuda", local))
-    else:
-        torch.cuda.set_device(0)
-    allm = W.ensemble_members()[:a.members]
-    mine = [m for k, m in enumerate(allm) if k % world == rank]
-    ens = build_ensemble(mine, "f32")
+    ens = build_ensemble(members, "f32")
     ens.step(1)
     variant, vms = ens.autotune(5)
     ens.step(a.warmup)
@@ -444,25 +436,20 @@ def ensemble_bench(a):
     ens.set_graph(0)
     ms_nograph = timed(ens.step, a.steps)
     ens.set_graph(_lib.LBM_ENS_GRAPH_STEPS)
+    k_step, k_bc = ens.profile(a.steps)
 
     def sequential(n):
         for L in ens.members:
             L.step(n)
     ms_seq = timed(sequential, a.steps)
     st = max(L.status() for L in ens.members)
-    cells = sum(m.cells for m in allm)
-    mlups = lambda t: cells * a.steps / (t * 1e-3) / 1e6
+    ens.close()
+    cells = sum(m.cells for m in members)
     hbm, hbm_kind = peaks()
-    achieved = cells * bytes_per_lup(19, "f32") / (ms / a.steps * 1e-3) / 1e9
-    line = {"metric": "aggregate MLUPS of a batched ensemble vs the same members run one after another",
-            "value": round(mlups(ms), 1), "unit": "MLUPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic (seeded member sizes, inflow speeds and inflow-turbulence fields)",
-            "config": {"workload": "ensemble_q19_64_members", "members": len(allm), "cells": cells,
-                       "sizes": "nx in [96,192], ny, nz in [48,96], multiples of 8 (seeded)",
-                       "physics": "D3Q19 FP32 regularized + Vreman, inflow U[0.03,0.07], turbulence ampl 1e-4 at i=10",
-                       "parallelism": "members round-robin over %d GPU(s)" % world if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2: %.1f GB of state" % (cells * 19 * 4 * 2 / 1e9)},
+    bl = bytes_per_lup(19, "f32")
+    mlups = lambda t: cells * a.steps / (t * 1e-3) / 1e6
+    return {"value": round(mlups(ms), 1), "unit": "MLUPS", "ms_per_step": round(ms / a.steps, 4), "cells": cells,
+            "members": len(members),
             "batched": {"launches_per_step": 2, "graph_steps": _lib.LBM_ENS_GRAPH_STEPS,
                         "autotune": {"variant": variant, "threads_per_block": _lib.ENS_THREADS[variant],
                                      "ms_per_step": [round(x, 4) for x in vms]}},
@@ -470,11 +457,45 @@ def ensemble_bench(a):
             "sequential": {"value": round(mlups(ms_seq), 1), "ms_per_step": round(ms_seq / a.steps, 4),
                            "how": "lbm_step on each member's context in turn, %d steps each" % a.steps},
             "speedup_vs_sequential": round(ms_seq / ms, 3),
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": hbm_kind,
-                         "note": "whole step (both launches), 152 B per cell update"},
-            "gpu_launches": 2 * a.steps, "clocks": clk.report(), "status_flags": st}
-    ens.close()
+            "roofline": {"bound": "hbm", "achieved": round(cells * bl / (k_step * 1e-3) / 1e9, 1), "peak": hbm,
+                         "unit": "GB/s", "frac": round(cells * bl / (k_step * 1e-3) / 1e9 / hbm, 4),
+                         "peak_kind": hbm_kind, "kernel": "k_ens_step<19,float>", "kernel_ms": round(k_step, 4),
+                         "boundary_kernel_ms": round(k_bc, 4),
+                         "step_frac": round(cells * bl / (ms / a.steps * 1e-3) / 1e9 / hbm, 4),
+                         "note": "frac: the step kernel alone (CUDA events around each launch, %d direct-launch "
+                                 "steps); step_frac: the whole graph-replayed step, 152 B per cell update" % a.steps},
+            "clocks": clk.report(), "status_flags": st}
+
+
+def ensemble_bench(a):
+    """The batched-ensemble benchmark as its own JSON line.  Under torchrun the
+    members are dealt out round-robin to the ranks (independent replicas)."""
+    import torch
+    from lbm_b200 import replicas, workloads as W
+    rank, local, world = replicas.env_rank()
+    dist = None
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist = replicas.init("nccl", timeout_s=300, device=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    allm = W.ensemble_members()[:a.members]
+    mine = [m for k, m in enumerate(allm) if k % world == rank]
+    r = ensemble_measure(a, mine, dist)
+    cells = sum(m.cells for m in allm)
+    line = {"metric": "aggregate MLUPS of a batched ensemble vs the same members run one after another",
+            "value": round(cells / (r["ms_per_step"] * 1e-3) / 1e6, 1),   # every rank's members, max-over-ranks time
+            "unit": "MLUPS", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (seeded member sizes, inflow speeds and inflow-turbulence fields)",
+            "config": {"workload": "ensemble_q19_%d_members" % len(allm), "members": len(allm), "cells": cells,
+                       "sizes": "nx in [96,192], ny, nz in [48,96], multiples of 8 (seeded)",
+                       "physics": "D3Q19 FP32 regularized + Vreman, inflow U[0.03,0.07], turbulence ampl 1e-4 at i=10",
+                       "parallelism": "members round-robin over %d GPU(s)" % world if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2: %.1f GB of state" % (cells * 19 * 4 * 2 / 1e9)},
+            "gpu_launches": 2 * a.steps}
+    for k in ("batched", "no_graph", "sequential", "speedup_vs_sequential", "roofline", "clocks", "status_flags"):
+        line[k] = r[k]
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -910,6 +931,9 @@ def main():
 
     if not a.no_q19 and world == 1 and wl.name == W.CHANNEL_Q27.name:
         line["q19"] = lattice_leg(a, W.CHANNEL_Q19, hbm)
+    if not a.no_ens and world == 1 and wl.name == W.CHANNEL_Q27.name:
+        line["ensemble"] = dict(workload="ensemble_q19_64_members", **ensemble_measure(a, W.ensemble_members()))
+        torch.cuda.empty_cache()
 
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)

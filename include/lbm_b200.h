@@ -391,6 +391,10 @@ int lbm_ensemble_step(lbm_ensemble* ens, int32_t nsteps);
  * ms_per_step[LBM_ENS_VARIANTS] may be NULL. */
 int lbm_ensemble_autotune(lbm_ensemble* ens, int32_t trial_steps, int32_t* variant, float* ms_per_step);
 int lbm_ensemble_set_variant(lbm_ensemble* ens, int32_t variant);
+/* advance nsteps batched steps with direct launches (no graph), timing every
+ * launch with CUDA events; returns the mean duration of the step kernel and of
+ * the boundary kernel in ms.  Synchronises the ensemble's stream. */
+int lbm_ensemble_profile(lbm_ensemble* ens, int32_t nsteps, float* step_kernel_ms, float* boundary_kernel_ms);
 /* steps per captured graph: 0 = direct launches, else a positive even count */
 int lbm_ensemble_set_graph(lbm_ensemble* ens, int32_t graph_steps);
 

@@ -366,6 +366,13 @@ module lbm_b200_iface
          integer(c_int32_t)        :: variant
          real(c_float)             :: ms_per_step(*)
       end function
+      integer(c_int) function lbm_ensemble_profile(ens, nsteps, step_kernel_ms, boundary_kernel_ms) &
+            bind(C, name="lbm_ensemble_profile")
+         import :: c_ptr, c_int, c_int32_t, c_float
+         type(c_ptr), value        :: ens
+         integer(c_int32_t), value :: nsteps
+         real(c_float)             :: step_kernel_ms, boundary_kernel_ms
+      end function
       integer(c_int) function lbm_ensemble_size(ens, nmembers) bind(C, name="lbm_ensemble_size")
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value  :: ens

@@ -129,6 +129,7 @@ SIGNATURES = {
     "lbm_ensemble_step": [P, I],
     "lbm_ensemble_autotune": [P, I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_variant": [P, I],
+    "lbm_ensemble_profile": [P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_graph": [P, I],
 }
 

@@ -490,6 +490,13 @@ class Ensemble:
     def set_variant(self, v: int):
         self._call("lbm_ensemble_set_variant", int(v))
 
+    def profile(self, nsteps: int):
+        """nsteps direct-launch steps timed launch by launch: (step-kernel ms,
+        boundary-kernel ms), the means per step."""
+        a, b = ctypes.c_float(0.0), ctypes.c_float(0.0)
+        self._call("lbm_ensemble_profile", int(nsteps), ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
     def set_graph(self, steps: int):
         self._call("lbm_ensemble_set_graph", int(steps))
 

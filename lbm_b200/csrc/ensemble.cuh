@@ -24,6 +24,7 @@ struct EnsMember {
     StepArgs a[2];       // arguments of a step whose source is buffer p (p = parity)
     void* buf[2];
     int nface_blocks;    // k_bc_fold layout of this member (blocks of 128 threads)
+    FastDiv hp, ny;      // division by the pairs per row (nx / 2) and by ny: the pair decode
 };
 
 struct EnsLayout {
@@ -46,13 +47,15 @@ __global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
     const EnsMember* em = L.mem + mb.x;
     ens_load_args(raw, &em->a[parity]);
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
-    const int hp = a.g.nx / 2;
-    const long long q = (long long)mb.y * T + threadIdx.x;
-    if (q >= (long long)hp * a.g.ny * a.g.nz) return;
-    const int row = (int)(q / hp);
-    const int i = 2 * (int)(q - (long long)row * hp) + 1;
-    const int j = row % a.g.ny + 1;
-    const int k = row / a.g.ny + 1;
+    // 32-bit decode by multiply-high (a member holds fewer than 2^31 pairs)
+    const unsigned hp = (unsigned)(a.g.nx / 2);
+    const unsigned q = (unsigned)mb.y * T + threadIdx.x;
+    if (q >= hp * (unsigned)a.g.ny * (unsigned)a.g.nz) return;
+    const unsigned row = fdiv(q, em->hp);
+    const int i = 2 * (int)(q - row * hp) + 1;
+    const unsigned kk = fdiv(row, em->ny);
+    const int j = (int)(row - kk * (unsigned)a.g.ny) + 1;
+    const int k = (int)kk + 1;
     const S* src = reinterpret_cast<const S*>(em->buf[parity]);
     S* dst = reinterpret_cast<S*>(em->buf[1 - parity]);
     pair_cell<Q, S, true>(src, dst, a, i, j, k);

@@ -82,29 +82,37 @@ int ens_upload(lbm_ensemble* e) {
         d.buf[0] = c->buf[0];
         d.buf[1] = c->buf[1];
         d.nface_blocks = bc_fold_face_blocks(c->sg);
+        d.hp = make_fastdiv((unsigned)(c->sg.nx / 2));
+        d.ny = make_fastdiv((unsigned)c->sg.ny);
     }
     return echeck(e, cudaMemcpyAsync(e->d_mem, e->h_mem.data(), e->h_mem.size() * sizeof(EnsMember),
                                      cudaMemcpyHostToDevice, e->stream), "ensemble descriptors");
 }
 
+// one batched step: the step kernel, then the boundary kernel; ev (or null): events
+// recorded before the step kernel, between the two and after the boundary kernel
 template <int Q, typename S>
-int ens_launch_step(lbm_ensemble* e, int parity) {
+int ens_launch_step(lbm_ensemble* e, int parity, cudaEvent_t* ev) {
     const EnsLayout Ls = ens_layout(e, e->variant);
     const int nb = e->nblk[e->variant];
+    if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[0], e->stream), "ensemble profile"));
     switch (kEnsThreads[e->variant]) {
         case 64: k_ens_step<Q, S, 64, 10><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
         case 128: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
         default: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
     }
     LBM_TRY(echeck(e, cudaGetLastError(), "ensemble step"));
+    if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[1], e->stream), "ensemble profile"));
     k_ens_bc<Q, S><<<e->nblk[LBM_ENS_VARIANTS], 128, 0, e->stream>>>(ens_layout(e, LBM_ENS_VARIANTS), parity);
-    return echeck(e, cudaGetLastError(), "ensemble boundaries");
+    LBM_TRY(echeck(e, cudaGetLastError(), "ensemble boundaries"));
+    if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[2], e->stream), "ensemble profile"));
+    return LBM_OK;
 }
 
-int ens_launch(lbm_ensemble* e, int parity) {
+int ens_launch(lbm_ensemble* e, int parity, cudaEvent_t* ev = nullptr) {
     const bool h = e->storage == LBM_STORE_F16;
-    if (e->nl == 27) return h ? ens_launch_step<27, __half>(e, parity) : ens_launch_step<27, float>(e, parity);
-    return h ? ens_launch_step<19, __half>(e, parity) : ens_launch_step<19, float>(e, parity);
+    if (e->nl == 27) return h ? ens_launch_step<27, __half>(e, parity, ev) : ens_launch_step<27, float>(e, parity, ev);
+    return h ? ens_launch_step<19, __half>(e, parity, ev) : ens_launch_step<19, float>(e, parity, ev);
 }
 
 int ens_graph(lbm_ensemble* e) {
@@ -157,15 +165,20 @@ int ens_align(lbm_ensemble* e, int* used) {
     return LBM_OK;
 }
 
-// n batched steps on the ensemble stream, ordered after and before the members' stream
-int ens_run(lbm_ensemble* e, int n, bool allow_graph) {
+// n batched steps on the ensemble stream, ordered after and before the members' stream;
+// prof (or null): three events per step (ens_launch_step), direct launches only
+int ens_run(lbm_ensemble* e, int n, bool allow_graph, cudaEvent_t* prof = nullptr) {
     cudaStream_t ms = e->m[0]->stream;
     LBM_TRY(echeck(e, cudaEventRecord(e->ev[0], ms), "ensemble order"));
     LBM_TRY(echeck(e, cudaStreamWaitEvent(e->stream, e->ev[0], 0), "ensemble order"));
     LBM_TRY(ens_upload(e));
     int left = n;
     while (left > 0) {
-        if (allow_graph && e->graph_steps > 0 && e->cur == 0 && left >= e->graph_steps) {
+        if (prof) {
+            LBM_TRY(ens_launch(e, e->cur, prof + 3 * (n - left)));
+            e->cur ^= 1;
+            left -= 1;
+        } else if (allow_graph && e->graph_steps > 0 && e->cur == 0 && left >= e->graph_steps) {
             LBM_TRY(ens_graph(e));
             LBM_TRY(echeck(e, cudaGraphLaunch(e->graph, e->stream), "graph launch"));
             left -= e->graph_steps;   // an even count: the parity is back to 0
@@ -231,6 +244,7 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
                 long long nb;
                 if (v < LBM_ENS_VARIANTS) {
                     const long long pairs = (long long)(g.nx / 2) * g.ny * g.nz;
+                    if (pairs >= (1LL << 31)) rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: 2^31 pairs or more", (int)k);
                     nb = (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
@@ -315,6 +329,32 @@ int lbm_ensemble_set_graph(lbm_ensemble* e, int32_t graph_steps) {
     }
     e->graph_steps = graph_steps;
     return LBM_OK;
+}
+
+int lbm_ensemble_profile(lbm_ensemble* e, int32_t nsteps, float* step_kernel_ms, float* boundary_kernel_ms) {
+    if (!e || nsteps < 1 || !step_kernel_ms || !boundary_kernel_ms) return LBM_ERR_ARG;
+    int used = 0;
+    LBM_TRY(ens_align(e, &used));
+    std::vector<cudaEvent_t> ev(3 * (size_t)nsteps, nullptr);
+    int rc = LBM_OK;
+    for (size_t q = 0; q < ev.size() && rc == LBM_OK; ++q) rc = echeck(e, cudaEventCreate(&ev[q]), "cudaEventCreate");
+    if (rc == LBM_OK) rc = ens_run(e, nsteps, false, ev.data());
+    if (rc == LBM_OK) rc = echeck(e, cudaEventSynchronize(ev.back()), "ensemble profile");
+    double ks = 0.0, kb = 0.0;
+    for (int s = 0; s < nsteps && rc == LBM_OK; ++s) {
+        float a = 0.f, b = 0.f;
+        rc = echeck(e, cudaEventElapsedTime(&a, ev[3 * s], ev[3 * s + 1]), "ensemble profile");
+        if (rc == LBM_OK) rc = echeck(e, cudaEventElapsedTime(&b, ev[3 * s + 1], ev[3 * s + 2]), "ensemble profile");
+        ks += a;
+        kb += b;
+    }
+    for (cudaEvent_t v : ev)
+        if (v) cudaEventDestroy(v);
+    if (rc == LBM_OK) {
+        *step_kernel_ms = (float)(ks / nsteps);
+        *boundary_kernel_ms = (float)(kb / nsteps);
+    }
+    return rc;
 }
 
 int lbm_ensemble_autotune(lbm_ensemble* e, int32_t trial_steps, int32_t* variant, float* ms_per_step) {

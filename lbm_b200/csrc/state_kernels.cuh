@@ -29,6 +29,26 @@
 
 namespace lbm {
 
+// n / d for 0 <= n < 2^31 by a multiply-high and a shift (Granlund-Montgomery
+// round-up method: m = ceil(2^(31+l) / d), l = ceil(log2 d), shift l - 1); d = 1
+// is the identity
+struct FastDiv {
+    unsigned d, m;
+    int s;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+    FastDiv f;
+    f.d = d < 1u ? 1u : d;
+    int l = 0;
+    while ((1ull << l) < f.d) ++l;
+    f.m = f.d == 1u ? 0u : (unsigned)(((1ull << (31 + l)) + f.d - 1) / f.d);
+    f.s = l > 0 ? l - 1 : 0;
+    return f;
+}
+__device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
+    return f.d == 1u ? n : (__umulhi(n, f.m) >> f.s);
+}
+
 struct StepArgs {
     SoaGrid g;
     CollideParams cp;
@@ -187,16 +207,25 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
         }
         return;
     }
-    // x-ghost threads: blocks of 128 j, then the direction l, then k (32-bit decode of the block index)
-    const int vbx = vb - nface_blocks;
-    const int nbj = (g.ny + 127) / 128;
-    const int rest = vbx / nbj;
-    const int j = (vbx - rest * nbj) * 128 + threadIdx.x + 1;
-    const int l = rest % Q;
-    const int k = rest / Q + 1;
-    if (vbx == 0 && threadIdx.x == 0) *a.d_it_rw += 1;   // the step counter advances once per step
-    if (j > g.ny || k > g.nz) return;
+    // x-ghost threads, one per (j, l, k), j fastest, packed (no idle threads for short rows);
+    // 32-bit index arithmetic where the count allows (it does up to 2^31 elements)
     const long long nyz = (long long)g.ny * g.nz;
+    const long long ne = (long long)Q * nyz;
+    const long long e = (long long)(vb - nface_blocks) * 128 + threadIdx.x;
+    if (e >= ne) return;
+    if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
+    int j, l, k;
+    if (ne < (1LL << 31)) {
+        const unsigned ue = (unsigned)e, uny = (unsigned)g.ny;
+        const unsigned r = ue / uny;
+        j = (int)(ue - r * uny) + 1;
+        l = (int)(r % (unsigned)Q);
+        k = (int)(r / (unsigned)Q) + 1;
+    } else {
+        j = (int)(e % g.ny) + 1;
+        l = (int)((e / g.ny) % Q);
+        k = (int)(e / ((long long)g.ny * Q)) + 1;
+    }
     const int cx = c_cx[l], cy = c_cy[l], cz = c_cz[l];
     S* fl = f1 + (long long)l * g.dstride;
     if (k == 1 || k == g.nz) {
@@ -241,7 +270,7 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
 // blocks of bc_fold_block: the k-face blocks, then the x-ghost blocks
 __host__ __device__ inline int bc_fold_face_blocks(const SoaGrid& g) { return 2 * g.ny * ((g.nx + 127) / 128); }
 __host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q) {
-    return (long long)((g.ny + 127) / 128) * Q * g.nz;
+    return ((long long)Q * g.ny * g.nz + 127) / 128;
 }
 
 // Programmatic dependent launch (PDL) between the steady step kernel and the
