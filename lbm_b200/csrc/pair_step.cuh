@@ -403,8 +403,8 @@ __device__ __forceinline__ void pair_edge(const f2 (&fp)[Q], const StepArgs& a, 
         S* e = (S*)a.edge + (long long)c * Q * nyz + (long long)(k - 1) * a.g.ny + (j - 1);
 #pragma unroll
         for (int l = 0; l < Q; ++l) {
-            if constexpr (sizeof(S) == 2) __stwb(e + l * nyz, __float2half_rn(comp(fp[l], c)));   // already 2^8-scaled
-            else __stwb(e + l * nyz, comp(fp[l], c));
+            if constexpr (sizeof(S) == 2) e[l * nyz] = __float2half_rn(comp(fp[l], c));   // already 2^8-scaled
+            else e[l * nyz] = comp(fp[l], c);
         }
     }
 }
@@ -418,11 +418,9 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
     S* q = dst + o;
 #pragma unroll
     for (int l = 0; l < Q; ++l) {
-        // global-space stores (st.global) also where the destination pointer comes from
-        // shared memory (the ensemble kernel), which the compiler cannot place
         char* qb = reinterpret_cast<char*>(q) + a.soffb[l];
-        if constexpr (sizeof(S) == 2) __stwb(reinterpret_cast<__half2*>(qb), __floats2half2_rn(fp[l].x, fp[l].y));
-        else __stwb(reinterpret_cast<float2*>(qb), fp[l]);
+        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
+        else *reinterpret_cast<float2*>(qb) = fp[l];
     }
     if (FOLD) pair_edge<Q, S>(fp, a, i, j, k);
 }
