@@ -511,7 +511,7 @@ int step_one(lbm_ctx* c) {
         }
         LBM_TRY(prof_end(c));
         const int nface = bc_fold_face_blocks(g);
-        const int nblk = nface + (int)bc_fold_xg_blocks(g, Q);
+        const int nblk = nface + (int)bc_fold_xg_blocks(g, Q, false);
         LBM_TRY(cuda_check(c, launch_pdl(k_bc_fold<Q, S>, dim3(nblk), dim3(128), c->stream, (S*)c->buf[nxt],
                                          (const S*)c->buf[c->cur], a, nface), "folded boundaries"));
         c->launches++;

@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(128) k_ens_bc(EnsLayout L, int parity) {
     const EnsMember* em = L.mem + mb.x;
     ens_load_args(raw, &em->a[parity]);
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
-    bc_fold_block<Q, S>(reinterpret_cast<S*>(em->buf[1 - parity]), reinterpret_cast<const S*>(em->buf[parity]), a,
+    bc_fold_block<Q, S, true>(reinterpret_cast<S*>(em->buf[1 - parity]), reinterpret_cast<const S*>(em->buf[parity]), a,
                         em->nface_blocks, mb.y);
 }
 

@@ -248,7 +248,7 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
                     nb = (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
-                    nb = bc_fold_face_blocks(g) + bc_fold_xg_blocks(g, e->nl);
+                    nb = bc_fold_face_blocks(g) + bc_fold_xg_blocks(g, e->nl, true);
                 }
                 for (long long b = 0; b < nb; ++b) blk.push_back(make_int2((int)k, (int)b));
             }

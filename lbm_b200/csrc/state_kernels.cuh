@@ -166,54 +166,128 @@ __device__ __forceinline__ void store_sector(S* p, S v, int slot) {
     q[1] = make_uint4(w[4], w[5], w[6], w[7]);
 }
 
+// The inflow ghost value of a direction whose source is the post-collision
+// value fin of direction ls (weight wl, velocity (cx, cy)) at the cell i = 1,
+// with uu the inflow speed of the cell's k (m_boundary_i_inflow_kernel.F90:
+// 56-111): fin - 2 wl rho0 (cx uu cos + cy uu sin) / cs2, rounded operation by
+// operation in that order.
+__device__ __forceinline__ float inflow_value(float fin, float wl, int cx, int cy, float uu, const StepArgs& a) {
+    const float t = __fadd_rn(__fmul_rn(__fmul_rn((float)cx, uu), a.cosd), __fmul_rn(__fmul_rn((float)cy, uu), a.sind));
+    const float p = __fmul_rn(__fmul_rn(__fmul_rn(2.0f, wl), a.rho0), t);
+    return __fsub_rn(fin, __fdiv_rn(p, 1.0f / 3.0f));
+}
+
 // Boundary kernel of the folded configuration, run after k_step on the new
-// buffer f1 (= dst of the step) with f2 the old buffer.  Two kinds of threads:
+// buffer f1 (= dst of the step) with f2 the old buffer.  Two kinds of threads,
+// each issuing all its loads before its first store (the stores go to ghost
+// cells none of its loads reads, but the compiler cannot prove it), so that a
+// thread waits on memory once:
 //   * k-face threads, one per (i, j, face) with i in 1..nx: for each outgoing
 //     direction l of the face, f1(l,i,j,kg) = f1(l, i-cx, j-cy, kp) when the
 //     source is an interior cell, and f1(m,i,j,kg) = f2(l,i,j,kg) for the
 //     reflected direction m (m_boundary_k_closed_kernel.F90:35-46).
-//   * x-ghost threads, one per (l, j, k): the inflow value of ghost (0,j,k)
-//     and the outflow value of ghost (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:
-//     184-231), written to the compact x-ghost array, and into the rows for
-//     the directions the next pull reads there.  At the planes k=1 and k=nz
-//     they first pass the value their x-ghost held before this step to the
-//     k-ghost cell that the reference's k-face copies it to (sources i-cx = 0
-//     or nx+1; always a pulled direction, so it is in the rows), so each
-//     x-ghost element is read and then written by one and the same thread.
+//   * x-ghost threads: the inflow ghost (0,j,k) and the outflow ghost
+//     (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:184-231), written to the
+//     compact x-ghost array, and into the rows for the directions the next pull
+//     reads there (cx > 0 at i = 0, cx < 0 at nx+1).  At the planes k=1 and
+//     k=nz they first pass the value those row ghosts held before this step to
+//     the k-ghost cell that the reference's k-face copies it to (1 or nx, j+cy,
+//     kg), so each ghost is read and then written by one and the same thread.
+//     WIDE: one thread per (j, k, side) with every direction (fewer, longer
+//     threads: faster for the short columns of small ensemble members); else
+//     one thread per (j, l, k), both sides (faster for large domains).
 // vb: this block's index among the nface_blocks + x-ghost blocks of the grid
 // (blocks of 128 threads).
-template <int Q, typename S>
-__device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs& a, int nface_blocks, int vb) {
+template <int Q, typename S, int SIDE>
+__device__ __forceinline__ void bc_fold_face(S* f1, const S* f2, const SoaGrid& g, int opt, int i, int j) {
+    constexpr int NO = (Q == 27) ? 9 : 5;   // outgoing directions of a face
+    const int kp = SIDE ? g.nz : 1, kg = SIDE ? g.nz + 1 : 0;
+    const long long og = g.off(i, j, kg);
+    S cp[NO], rf[NO];
+    bool in[NO];
+    int n = 0;
+#pragma unroll
+    for (int l = 1; l < Q; ++l) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        if (SIDE ? (cz <= 0) : (cz >= 0)) continue;
+        const int si = i - cx;
+        in[n] = si >= 1 && si <= g.nx;
+        if (in[n]) cp[n] = f1[(long long)l * g.dstride + g.off(si, wrapj(j - cy, g.ny), kp)];
+        rf[n] = f2[(long long)l * g.dstride + og];
+        ++n;
+    }
+    n = 0;
+#pragma unroll
+    for (int l = 1; l < Q; ++l) {
+        const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
+        if (SIDE ? (cz <= 0) : (cz >= 0)) continue;
+        if (in[n]) f1[(long long)l * g.dstride + og] = cp[n];
+        const int m = opt < 0 ? lat_opposite(l) : lat_find<Q>(cx, cy, -cz);
+        f1[(long long)m * g.dstride + og] = rf[n];
+        ++n;
+    }
+}
+
+template <int Q, typename S, int SIDE>
+__device__ __forceinline__ void bc_fold_xcol(S* f1, const StepArgs& a, int j, int k, long long cell) {
     const SoaGrid& g = a.g;
-    if (vb < nface_blocks) {
-        const int per_row = (g.nx + 127) / 128;
-        const int b = vb;
-        const int side = b / (per_row * g.ny);
-        const int j = (b / per_row) % g.ny + 1;
-        const int i = (b % per_row) * 128 + threadIdx.x + 1;
-        if (i > g.nx) return;
-        const int kp = side ? g.nz : 1, kg = side ? g.nz + 1 : 0;
-        const int opt = side ? a.kopt_hi : a.kopt_lo;
+    const long long nyz = (long long)g.ny * g.nz;
+    const S* edge = (const S*)a.edge + (long long)SIDE * Q * nyz + cell;   // cell 1 (side 0) or nx (side 1)
+    S* xg = (S*)a.xg_dst + (long long)SIDE * Q * nyz + cell;                 // xg_index(g, Q, SIDE, l, j, k)
+    const int ig = SIDE ? g.nx + 1 : 0;   // the ghost column
+    S ev[Q];
+#pragma unroll
+    for (int l = 0; l < Q; ++l) ev[l] = edge[l * nyz];
+    const float uu = SIDE ? 0.0f : a.uvel[k - 1];
+    if (k == 1 || k == g.nz) {
+        constexpr int NS = (Q == 27) ? 9 : 5;   // directions the pull reads at this ghost
+        const int kg = (k == 1) ? 0 : g.nz + 1;
+        const int ib = SIDE ? g.nx : 1;
+        S old[NS];
+        int n = 0;
 #pragma unroll
         for (int l = 1; l < Q; ++l) {
-            const int cx = lat_cx(l), cy = lat_cy(l), cz = lat_cz(l);
-            const bool out = side ? (cz > 0) : (cz < 0);
-            if (!out) continue;
-            const int si = i - cx;
-            if (si >= 1 && si <= g.nx)
-                f1[(long long)l * g.dstride + g.off(i, j, kg)] = f1[(long long)l * g.dstride + g.off(si, wrapj(j - cy, g.ny), kp)];
-            const int m = opt < 0 ? lat_opposite(l) : lat_find<Q>(cx, cy, -cz);
-            f1[(long long)m * g.dstride + g.off(i, j, kg)] = f2[(long long)l * g.dstride + g.off(i, j, kg)];
+            if (SIDE ? (lat_cx(l) >= 0) : (lat_cx(l) <= 0)) continue;
+            old[n++] = f1[(long long)l * g.dstride + g.off(ig, j, k)];
         }
-        return;
+        n = 0;
+#pragma unroll
+        for (int l = 1; l < Q; ++l) {
+            const int cy = lat_cy(l), cz = lat_cz(l);
+            if (SIDE ? (lat_cx(l) >= 0) : (lat_cx(l) <= 0)) continue;
+            if ((k == 1) ? (cz < 0) : (cz > 0)) f1[(long long)l * g.dstride + g.off(ib, wrapj(j + cy, g.ny), kg)] = old[n];
+            ++n;
+        }
     }
-    // x-ghost threads, one per (j, l, k), j fastest, packed (no idle threads for short rows);
-    // 32-bit index arithmetic where the count allows (it does up to 2^31 elements)
+    constexpr int spe = 32 / (int)sizeof(S);
+#pragma unroll
+    for (int l = 0; l < Q; ++l) {
+        S v;
+        if (SIDE == 0) {
+            // directions with cx > 0 take the corrected value of their opposite
+            const int ls = lat_cx(l) > 0 ? lat_opposite(l) : l;
+            v = Store<S>::from_f(inflow_value(Store<S>::to_f(ev[ls]), lat_w<Q>(ls), lat_cx(ls), lat_cy(ls), uu, a));
+        } else {
+            v = ev[l];   // zero gradient
+        }
+        xg[l * nyz] = v;
+        // the rows: a ghost's 32-byte sector holds nothing else but row padding, so
+        // it is written whole (no read-modify-write of a partial sector)
+        if (SIDE ? (lat_cx(l) < 0) : (lat_cx(l) > 0)) {
+            S* p = f1 + (long long)l * g.dstride + g.off(ig, j, k);
+            if (a.full_sector) store_sector<S>(SIDE ? p : p - (spe - 1), v, SIDE ? 0 : spe - 1);
+            else *p = v;
+        }
+    }
+}
+
+// one x-ghost thread per (j, l, k), both sides (j fastest, packed: no idle
+// threads for short rows; 32-bit index arithmetic up to 2^31 elements)
+template <int Q, typename S>
+__device__ __forceinline__ void bc_fold_xelem(S* f1, const StepArgs& a, long long e) {
+    const SoaGrid& g = a.g;
     const long long nyz = (long long)g.ny * g.nz;
     const long long ne = (long long)Q * nyz;
-    const long long e = (long long)(vb - nface_blocks) * 128 + threadIdx.x;
-    if (e >= ne) return;
-    if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
     int j, l, k;
     if (ne < (1LL << 31)) {
         const unsigned ue = (unsigned)e, uny = (unsigned)g.ny;
@@ -229,7 +303,6 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
     const int cx = c_cx[l], cy = c_cy[l], cz = c_cz[l];
     S* fl = f1 + (long long)l * g.dstride;
     if (k == 1 || k == g.nz) {
-        // stale x-ghost values feed the k-face ghost cells (1,.,kg) and (nx,.,kg)
         const bool out = (k == 1) ? (cz < 0) : (cz > 0);
         if (out) {
             const int kg = (k == 1) ? 0 : g.nz + 1;
@@ -241,19 +314,13 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
     const long long cell = (long long)(k - 1) * g.ny + (j - 1);
     // inflow: directions with cx > 0 take the corrected value of their opposite
     const int ls = (cx > 0) ? c_opp[l] : l;
-    const float wl = c_w[Q == 27 ? 1 : 0][ls];
-    const float cxl = (float)c_cx[ls], cyl = (float)c_cy[ls];
-    const float uu = a.uvel[k - 1];
-    const float cs2 = 1.0f / 3.0f;
     const float fin = Store<S>::to_f(edge[(long long)ls * nyz + cell]);
-    const S gin = Store<S>::from_f(fin - 2.0f * wl * a.rho0 * (cxl * uu * a.cosd + cyl * uu * a.sind) / cs2);
+    const S gin = Store<S>::from_f(inflow_value(fin, c_w[Q == 27 ? 1 : 0][ls], c_cx[ls], c_cy[ls], a.uvel[k - 1], a));
     // outflow: zero gradient
     const S gout = edge[((long long)Q + l) * nyz + cell];
     S* xg = (S*)a.xg_dst;
     xg[xg_index(g, Q, 0, l, j, k)] = gin;
     xg[xg_index(g, Q, 1, l, j, k)] = gout;
-    // the rows: a ghost's 32-byte sector holds nothing else but row padding, so
-    // it is written whole (no read-modify-write of a partial sector)
     constexpr int spe = 32 / (int)sizeof(S);
     if (cx > 0) {
         S* p = fl + g.off(0, j, k);
@@ -267,10 +334,41 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
     }
 }
 
+template <int Q, typename S, bool WIDE>
+__device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs& a, int nface_blocks, int vb) {
+    const SoaGrid& g = a.g;
+    if (vb < nface_blocks) {
+        const int per_row = (g.nx + 127) / 128;
+        const int b = vb;
+        const int side = b / (per_row * g.ny);
+        const int j = (b / per_row) % g.ny + 1;
+        const int i = (b % per_row) * 128 + threadIdx.x + 1;
+        if (i > g.nx) return;
+        if (side) bc_fold_face<Q, S, 1>(f1, f2, g, a.kopt_hi, i, j);
+        else bc_fold_face<Q, S, 0>(f1, f2, g, a.kopt_lo, i, j);
+        return;
+    }
+    const long long nyz = (long long)g.ny * g.nz;
+    const long long e = (long long)(vb - nface_blocks) * 128 + threadIdx.x;
+    if (e >= (WIDE ? 2 : Q) * nyz) return;
+    if (e == 0) *a.d_it_rw += 1;   // the step counter advances once per step
+    if (!WIDE) {
+        bc_fold_xelem<Q, S>(f1, a, e);
+        return;
+    }
+    // side 0 for every (j, k), then side 1, j fastest
+    const int side = e >= nyz ? 1 : 0;
+    const long long cell = e - side * nyz;
+    const int j = (int)(cell % g.ny) + 1;
+    const int k = (int)(cell / g.ny) + 1;
+    if (side) bc_fold_xcol<Q, S, 1>(f1, a, j, k, cell);
+    else bc_fold_xcol<Q, S, 0>(f1, a, j, k, cell);
+}
+
 // blocks of bc_fold_block: the k-face blocks, then the x-ghost blocks
 __host__ __device__ inline int bc_fold_face_blocks(const SoaGrid& g) { return 2 * g.ny * ((g.nx + 127) / 128); }
-__host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q) {
-    return ((long long)Q * g.ny * g.nz + 127) / 128;
+__host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q, bool wide) {
+    return ((wide ? 2LL : (long long)Q) * g.ny * g.nz + 127) / 128;
 }
 
 // Programmatic dependent launch (PDL) between the steady step kernel and the
@@ -286,7 +384,7 @@ __device__ __forceinline__ void pdl_enter() {
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
     pdl_enter();
-    bc_fold_block<Q, S>(f1, f2, a, nface_blocks, blockIdx.x);
+    bc_fold_block<Q, S, false>(f1, f2, a, nface_blocks, blockIdx.x);
 }
 
 // The ghost cells of a state buffer, numbered t = 0 .. ghost_cells(g) - 1: whole
