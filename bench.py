@@ -241,7 +241,12 @@ def make_solver(wl, storage, seed, kernel=None):
 
 
 def timed_steps(s, steps, dist, profile=True):
-    """Time exactly `steps` fused steps with CUDA events on the library's stream; max over ranks."""
+    """Time exactly `steps` fused steps with CUDA events on the library's stream; max over ranks.
+    profile: the library also times every step kernel and the boundary launches
+    after it with its own events (the mean kernel duration for the roofline);
+    those events stand between consecutive launches and cost the launch
+    overlap, so the step rate is taken from a run without them (measure_steps).
+    Returns (ms, launches, step-kernel ms summed, step kernels timed, boundary ms summed)."""
     import torch
     from lbm_b200 import replicas
     L = s.lbm
@@ -259,11 +264,28 @@ def timed_steps(s, steps, dist, profile=True):
     ms = e0.elapsed_time(e1)
     launched = L.launches - n0
     kms, kn = L.profile_read() if profile else (0.0, 0)
+    bms = L.profile_read_boundary()[0] if profile else 0.0
     L.profile(False)
     if dist is not None:
         ms = replicas.max_over_ranks(ms, device="cuda")
         dist.barrier()
-    return ms, launched, kms, kn
+    return ms, launched, kms, kn, bms
+
+
+def measure_steps(s, steps, dist, clk_dev=None):
+    """The step rate from `steps` steps timed without per-kernel events (inside the
+    clock sampler when clk_dev is given), then the mean step-kernel duration from
+    `steps` more steps timed kernel by kernel.  Returns (ms, launches, kernel ms
+    summed, kernel launches, boundary ms summed, clock report or None)."""
+    clk = None
+    if clk_dev is not None:
+        with ClockSampler(clk_dev) as sampler:
+            ms, launched, _, _, _ = timed_steps(s, steps, dist, profile=False)
+        clk = sampler.report()
+    else:
+        ms, launched, _, _, _ = timed_steps(s, steps, dist, profile=False)
+    _, _, kms, kn, bms = timed_steps(s, steps, dist, profile=True)
+    return ms, launched, kms, kn, bms, clk
 
 
 def e2e_steps(s, steps, wl, dist):
@@ -412,13 +434,21 @@ def ensemble_measure(a, members, dist=None):
     from lbm_b200 import replicas
     from lbm_b200 import _lib
     from lbm_b200.ensemble import build_ensemble
+    from lbm_b200 import Ensemble
     ens = build_ensemble(members, "f32")
     ens.step(1)
-    variant, vms = ens.autotune(5)
-    if ens.members[0].it % 2:
-        ens.step(1)                          # the graph starts at parity 0
-    ens.step(_lib.LBM_ENS_GRAPH_STEPS)       # captures and instantiates the graph outside the timed region
-    ens.step(a.warmup)
+    variant, vms = ens.autotune(5)           # launch shape, then graph replay or direct launches
+    _, graph_steps = ens.config()
+
+    def prepare(g):
+        # the mode g (graph steps, 0 = direct), a graph captured outside the timed region
+        ens.set_graph(g)
+        if g:
+            if ens.members[0].it % 2:
+                ens.step(1)                  # graphs start at parity 0
+            ens.step(g)
+        ens.step(a.warmup)
+    prepare(graph_steps)
 
     def timed(fn, n):
         if dist is not None:
@@ -436,9 +466,10 @@ def ensemble_measure(a, members, dist=None):
 
     with ClockSampler(torch.cuda.current_device()) as clk:
         ms = timed(ens.step, a.steps)
-    ens.set_graph(0)
-    ms_nograph = timed(ens.step, a.steps)
-    ens.set_graph(_lib.LBM_ENS_GRAPH_STEPS)
+    other = 0 if graph_steps else _lib.LBM_ENS_GRAPH_STEPS
+    prepare(other)
+    ms_other = timed(ens.step, a.steps)
+    prepare(graph_steps)
     k_step, k_bc = ens.profile(a.steps)
 
     def sequential(n):
@@ -453,10 +484,15 @@ def ensemble_measure(a, members, dist=None):
     mlups = lambda t: cells * a.steps / (t * 1e-3) / 1e6
     return {"value": round(mlups(ms), 1), "unit": "MLUPS", "ms_per_step": round(ms / a.steps, 4), "cells": cells,
             "members": len(members),
-            "batched": {"launches_per_step": 2, "graph_steps": _lib.LBM_ENS_GRAPH_STEPS,
-                        "autotune": {"variant": variant, "threads_per_block": _lib.ENS_THREADS[variant],
-                                     "ms_per_step": [round(x, 4) for x in vms]}},
-            "no_graph": {"value": round(mlups(ms_nograph), 1), "ms_per_step": round(ms_nograph / a.steps, 4)},
+            "batched": {"launches_per_step": 2, "graph_steps": graph_steps,
+                        "autotune": {"variant": variant, "shape": Ensemble.variant_shape(variant),
+                                     "shapes": [Ensemble.variant_shape(v) for v in range(_lib.LBM_ENS_VARIANTS)],
+                                     "shape_ms_per_step": [round(x, 4) for x in vms],
+                                     "how": "each (threads per block, min blocks per SM) shape over 5 direct-launch "
+                                            "steps, then the fastest replayed from %d-step graphs vs launched "
+                                            "directly" % _lib.LBM_ENS_GRAPH_STEPS}},
+            ("direct_launches" if graph_steps else "graph_replay"):
+                {"value": round(mlups(ms_other), 1), "ms_per_step": round(ms_other / a.steps, 4)},
             "sequential": {"value": round(mlups(ms_seq), 1), "ms_per_step": round(ms_seq / a.steps, 4),
                            "how": "lbm_step on each member's context in turn, %d steps each" % a.steps},
             "speedup_vs_sequential": round(ms_seq / ms, 3),
@@ -497,8 +533,10 @@ def ensemble_bench(a):
                        "parallelism": "members round-robin over %d GPU(s)" % world if world > 1 else "single GPU",
                        "l2": "inputs larger than L2: %.1f GB of state" % (cells * 19 * 4 * 2 / 1e9)},
             "gpu_launches": 2 * a.steps}
-    for k in ("batched", "no_graph", "sequential", "speedup_vs_sequential", "roofline", "clocks", "status_flags"):
-        line[k] = r[k]
+    for k in ("batched", "direct_launches", "graph_replay", "sequential", "speedup_vs_sequential", "roofline",
+              "clocks", "status_flags"):
+        if k in r:
+            line[k] = r[k]
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -830,7 +868,7 @@ def lattice_leg(a, wl, hbm):
     for storage in ("f32", "f16"):
         s = make_solver(wl, storage, seed=wl.seed, kernel=a.kernel)
         s.step(a.warmup)
-        ms, _, kms, kn = timed_steps(s, a.steps, None)
+        ms, _, kms, kn, bms, _ = measure_steps(s, a.steps, None)
         st = s.lbm.status()
         s.close()
         del s
@@ -838,7 +876,8 @@ def lattice_leg(a, wl, hbm):
         k_ms = kms / max(kn, 1)
         bl = bytes_per_lup(wl.nl, storage)
         r = {"value": round(wl.cells * a.steps / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS",
-             "ms_per_step": round(ms / a.steps, 4), "kernel_ms": round(k_ms, 4), "bytes_per_lup": bl,
+             "ms_per_step": round(ms / a.steps, 4), "kernel_ms": round(k_ms, 4),
+             "boundary_kernel_ms": round(bms / max(kn, 1), 4), "bytes_per_lup": bl,
              "roofline_frac": round(wl.cells * bl / (k_ms * 1e-3) / 1e9 / hbm, 4) if kn else None,
              "status_flags": st}
         if storage == "f32":
@@ -882,8 +921,7 @@ def main():
     s = make_solver(wl, a.storage, seed=replicas.replica_seed(wl.seed, rank), kernel=a.kernel)
     s.step(a.warmup)
     torch.cuda.synchronize()
-    with ClockSampler(dev) as clk:
-        ms, launched, kms, kn = timed_steps(s, a.steps, dist)
+    ms, launched, kms, kn, bms, clocks = measure_steps(s, a.steps, dist, clk_dev=dev)
     st = s.lbm.status()
     cells = wl.cells
     value = world * cells * a.steps / (ms * 1e-3) / 1e6
@@ -903,10 +941,15 @@ def main():
                          "unit": "GB/s", "frac": round(achieved / hbm, 4) if achieved else None,
                          "traffic": traffic, "peak_kind": hbm_kind,
                          "kernel": key, "kernel_ms": round(k_ms, 4), "kernel_launches": kn,
+                         "boundary_kernel_ms": round(bms / max(kn, 1), 4),
                          "algorithmic_bytes_per_launch": cells * bl,
                          "frac_of_nominal_8000_gbs": round(achieved / NOMINAL_HBM_GBS, 4) if achieved else None,
-                         "note": "frac of %s HBM copy bandwidth; traffic = ncu dram bytes per launch" % hbm_kind},
-            "gpu_launches": launched, "clocks": clk.report(), "status_flags": st}
+                         "note": "frac of %s HBM copy bandwidth; kernel_ms and boundary_kernel_ms: mean "
+                                 "durations of the step kernel and of the boundary kernel after it (k_bc_fold), "
+                                 "over a second run of the same steps timed launch by launch (value and "
+                                 "ms_per_step come from the run without per-launch events); traffic = ncu dram "
+                                 "bytes per launch" % hbm_kind},
+            "gpu_launches": launched, "clocks": clocks, "status_flags": st}
 
     if not a.no_e2e:
         el, bad, h2d, d2h = e2e_steps(s, a.steps, wl, dist)
@@ -920,13 +963,15 @@ def main():
     if not a.no_f16 and a.storage == "f32" and world == 1:
         s16 = make_solver(wl, "f16", seed=replicas.replica_seed(wl.seed, rank), kernel=a.kernel)
         s16.step(a.warmup)
-        ms16, _, kms16, kn16 = timed_steps(s16, a.steps, dist)
+        ms16, _, kms16, kn16, bms16, _ = measure_steps(s16, a.steps, dist)
         s16.close()
         v16 = world * cells * a.steps / (ms16 * 1e-3) / 1e6
         ach16 = cells * bytes_per_lup(wl.nl, "f16") / (kms16 / max(kn16, 1) * 1e-3) / 1e9 if kn16 else None
         line["f16_storage"] = {"value": round(v16, 1), "unit": "MLUPS", "speedup_vs_f32": round(v16 / value, 3),
                                "roofline_frac": round(ach16 / hbm, 4) if ach16 else None,
-                               "kernel_ms": round(kms16 / max(kn16, 1), 4), "ms_per_step": round(ms16 / a.steps, 4)}
+                               "kernel_ms": round(kms16 / max(kn16, 1), 4),
+                               "boundary_kernel_ms": round(bms16 / max(kn16, 1), 4),
+                               "ms_per_step": round(ms16 / a.steps, 4)}
         torch.cuda.empty_cache()
         if not a.no_accuracy and wl.name == W.CHANNEL_Q27.name:
             # the stated-error half of the metric: the city workload after its 1000 steps

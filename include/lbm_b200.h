@@ -371,7 +371,7 @@ int lbm_state_adjoint_export(lbm_ctx* ctx, float* fhat, const float* A);
  * nx >= 4, and one lattice and storage for all. */
 typedef struct lbm_ensemble lbm_ensemble;
 enum {
-    LBM_ENS_VARIANTS = 3,      /* launch shapes of the step kernel: 64, 128, 256 threads per block */
+    LBM_ENS_VARIANTS = 6,      /* launch shapes of the step kernel: lbm_ensemble_variant_shape   */
     LBM_ENS_GRAPH_STEPS = 16   /* steps per captured graph (default; lbm_ensemble_set_graph)       */
 };
 int lbm_ensemble_create(lbm_ensemble** ens, const lbm_params* members, int32_t nmembers);
@@ -385,12 +385,22 @@ int lbm_ensemble_member(lbm_ensemble* ens, int32_t m, lbm_ctx** ctx);
  * their first step alone; all members must be imported before the first call
  * and afterwards be stepped only through the ensemble. */
 int lbm_ensemble_step(lbm_ensemble* ens, int32_t nsteps);
-/* time each launch shape over trial_steps steps and keep the fastest.  This
- * advances every member by LBM_ENS_VARIANTS * (trial_steps + 1) steps, plus the
- * first step of members imported since their last step.  variant and
- * ms_per_step[LBM_ENS_VARIANTS] may be NULL. */
+/* autotuner: time each launch shape over trial_steps steps (direct launches,
+ * one warm-up step each) and keep the fastest; then time that shape over
+ * LBM_ENS_GRAPH_STEPS steps replayed from a CUDA graph and as many launched
+ * directly, and keep the faster (graph_steps LBM_ENS_GRAPH_STEPS or 0, as
+ * lbm_ensemble_set_graph sets it).  This advances every member by
+ * LBM_ENS_VARIANTS * (trial_steps + 1) + 3 * LBM_ENS_GRAPH_STEPS steps, one more
+ * to bring the graphs to parity 0 where needed, plus the first step of members
+ * imported since their last step.  variant and ms_per_step[LBM_ENS_VARIANTS]
+ * (the shapes' times) may be NULL. */
 int lbm_ensemble_autotune(lbm_ensemble* ens, int32_t trial_steps, int32_t* variant, float* ms_per_step);
 int lbm_ensemble_set_variant(lbm_ensemble* ens, int32_t variant);
+/* the launch shape and graph steps in use (either pointer may be NULL) */
+int lbm_ensemble_get_config(const lbm_ensemble* ens, int32_t* variant, int32_t* graph_steps);
+/* launch shape `variant` of the step kernel: threads per block and the minimum
+ * resident blocks per SM it is compiled for (which caps its registers) */
+int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks);
 /* advance nsteps batched steps with direct launches (no graph), timing every
  * launch with CUDA events; returns the mean duration of the step kernel and of
  * the boundary kernel in ms.  Synchronises the ensemble's stream. */
@@ -401,10 +411,14 @@ int lbm_ensemble_set_graph(lbm_ensemble* ens, int32_t graph_steps);
 /* ---- instrumentation (no counterpart in the reference, whose timers are m_wtime.F90) ---- */
 /* number of kernel launches this context has issued */
 int lbm_launch_count(lbm_ctx* ctx, int64_t* n);
-/* enable (1) or disable (0) CUDA-event timing of every fused step-kernel launch; resets the totals */
+/* enable (1) or disable (0) CUDA-event timing of every steady step: its step
+ * kernel, and the boundary launches that follow it; resets the totals */
 int lbm_profile(lbm_ctx* ctx, int32_t enable);
 /* synchronise and return the summed device time and number of timed step-kernel launches */
 int lbm_profile_read(lbm_ctx* ctx, double* step_kernel_ms, int64_t* step_kernel_launches);
+/* synchronise and return the summed device time of the boundary launches of the
+ * timed steps (in the folded configuration: k_bc_fold) and the number of steps */
+int lbm_profile_read_boundary(lbm_ctx* ctx, double* boundary_ms, int64_t* steps);
 
 #ifdef __cplusplus
 }

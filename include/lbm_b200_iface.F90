@@ -383,6 +383,17 @@ module lbm_b200_iface
          type(c_ptr), value        :: ens
          integer(c_int32_t), value :: variant
       end function
+      integer(c_int) function lbm_ensemble_get_config(ens, variant, graph_steps) bind(C, name="lbm_ensemble_get_config")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value        :: ens
+         integer(c_int32_t)        :: variant, graph_steps
+      end function
+      integer(c_int) function lbm_ensemble_variant_shape(variant, threads, min_blocks) &
+            bind(C, name="lbm_ensemble_variant_shape")
+         import :: c_int, c_int32_t
+         integer(c_int32_t), value :: variant
+         integer(c_int32_t)        :: threads, min_blocks
+      end function
       integer(c_int) function lbm_ensemble_set_graph(ens, graph_steps) bind(C, name="lbm_ensemble_set_graph")
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value        :: ens
@@ -432,6 +443,13 @@ module lbm_b200_iface
          type(c_ptr), value  :: ctx
          real(c_double)      :: step_kernel_ms
          integer(c_int64_t)  :: step_kernel_launches
+      end function
+      integer(c_int) function lbm_profile_read_boundary(ctx, boundary_ms, steps) &
+            bind(C, name="lbm_profile_read_boundary")
+         import :: c_ptr, c_int, c_int64_t, c_double
+         type(c_ptr), value  :: ctx
+         real(c_double)      :: boundary_ms
+         integer(c_int64_t)  :: steps
       end function
    end interface
 end module lbm_b200_iface

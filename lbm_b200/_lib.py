@@ -27,9 +27,8 @@ LBM_STATUS_BAD_DENSITY = 1
 LBM_STATUS_TIMEOUT = 4
 LBM_KERNEL_PULL = 1
 LBM_KERNEL_PAIR = 2
-LBM_ENS_VARIANTS = 3
+LBM_ENS_VARIANTS = 6
 LBM_ENS_GRAPH_STEPS = 16
-ENS_THREADS = (64, 128, 256)      # threads per block of each ensemble launch shape
 
 
 class LbmParams(ctypes.Structure):
@@ -111,6 +110,7 @@ SIGNATURES = {
     "lbm_launch_count": [P, ctypes.POINTER(ctypes.c_int64)],
     "lbm_profile": [P, I],
     "lbm_profile_read": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],
+    "lbm_profile_read_boundary": [P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)],
     "lbm_inflow_turbulence_compute": [P, P, P, P, P, I, ctypes.c_uint64],
     "lbm_postcoll_adj": [P, P, P, P, P, P, P, P, P, P, P, P, P, P],
     "lbm_macrovars_adj": [P, P, P, P, P, P, P],
@@ -129,6 +129,8 @@ SIGNATURES = {
     "lbm_ensemble_step": [P, I],
     "lbm_ensemble_autotune": [P, I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_variant": [P, I],
+    "lbm_ensemble_get_config": [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+    "lbm_ensemble_variant_shape": [I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
     "lbm_ensemble_profile": [P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_graph": [P, I],
 }

@@ -448,6 +448,13 @@ class Lbm:
         self._call("lbm_profile_read", ctypes.byref(ms), ctypes.byref(n))
         return ms.value, n.value
 
+    def profile_read_boundary(self):
+        """(summed device ms, steps) of the boundary launches that followed the
+        timed step kernels since profile(True)."""
+        ms, n = ctypes.c_double(), ctypes.c_int64()
+        self._call("lbm_profile_read_boundary", ctypes.byref(ms), ctypes.byref(n))
+        return ms.value, n.value
+
 
 class Ensemble:
     """Many independent runs advanced together (``lbm_ensemble_*``): two launches
@@ -481,11 +488,28 @@ class Ensemble:
         self._call("lbm_ensemble_step", int(nsteps))
 
     def autotune(self, trial_steps: int = 5):
-        """Time each launch shape; returns (chosen variant, ms per step of each)."""
+        """Time each launch shape, then graph replay against direct launches for the
+        fastest; returns (chosen variant, ms per step of each shape)."""
         v = ctypes.c_int32(0)
         ms = (ctypes.c_float * _lib.LBM_ENS_VARIANTS)()
         self._call("lbm_ensemble_autotune", int(trial_steps), ctypes.byref(v), ms)
         return v.value, list(ms)
+
+    def config(self):
+        """(launch shape variant, graph steps: 0 = direct launches) in use."""
+        v, g = ctypes.c_int32(0), ctypes.c_int32(0)
+        self._call("lbm_ensemble_get_config", ctypes.byref(v), ctypes.byref(g))
+        return v.value, g.value
+
+    @staticmethod
+    def variant_shape(variant: int):
+        """(threads per block, minimum resident blocks per SM) of a launch shape."""
+        L = _lib.load()
+        t, m = ctypes.c_int32(0), ctypes.c_int32(0)
+        rc = L.lbm_ensemble_variant_shape(int(variant), ctypes.byref(t), ctypes.byref(m))
+        if rc != 0:
+            raise LbmError(rc, "variant %d out of range" % variant)
+        return t.value, m.value
 
     def set_variant(self, v: int):
         self._call("lbm_ensemble_set_variant", int(v))

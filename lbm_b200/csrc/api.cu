@@ -79,12 +79,14 @@ struct lbm_ctx {
     double* d_partial = nullptr;  // FP64 block partials of the conservation sums (scratch)
     double* d_sum = nullptr;      // their total (4 doubles)
     int it = 0;
-    // instrumentation: kernel launches issued, optional event timing of the step kernel
+    // instrumentation: kernel launches issued, optional event timing of the step
+    // kernel and of the boundary launches that follow it
     long long launches = 0;
     bool profiling = false;
-    std::vector<cudaEvent_t> ev;   // pairs (start, stop)
+    std::vector<cudaEvent_t> ev;   // triples (before the step kernel, after it, after the boundaries)
     size_t ev_used = 0;
     double prof_ms = 0.0;
+    double prof_bc_ms = 0.0;
     long long prof_launches = 0;
 };
 
@@ -117,28 +119,37 @@ int cuda_check(lbm_ctx* c, cudaError_t e, const char* what) {
 // left pending by earlier work of the calling thread is reported here and cleared too)
 #define LBM_LAUNCHED(c, what) LBM_TRY(cuda_check((c), cudaGetLastError(), (what)))
 
-// accumulate the elapsed time of recorded event pairs, then reuse them
+// accumulate the elapsed times of recorded event triples, then reuse them
 int prof_drain(lbm_ctx* c) {
     if (c->ev_used == 0) return LBM_OK;
-    int rc = cuda_check(c, cudaEventSynchronize(c->ev[2 * c->ev_used - 1]), "profile");
+    int rc = cuda_check(c, cudaEventSynchronize(c->ev[3 * c->ev_used - 1]), "profile");
     if (rc != LBM_OK) return rc;
     for (size_t q = 0; q < c->ev_used; ++q) {
-        float ms = 0.f;
-        rc = cuda_check(c, cudaEventElapsedTime(&ms, c->ev[2 * q], c->ev[2 * q + 1]), "profile");
+        float ms = 0.f, bc = 0.f;
+        rc = cuda_check(c, cudaEventElapsedTime(&ms, c->ev[3 * q], c->ev[3 * q + 1]), "profile");
+        if (rc == LBM_OK) rc = cuda_check(c, cudaEventElapsedTime(&bc, c->ev[3 * q + 1], c->ev[3 * q + 2]), "profile");
         if (rc != LBM_OK) return rc;
         c->prof_ms += ms;
+        c->prof_bc_ms += bc;
     }
     c->ev_used = 0;
     return LBM_OK;
 }
+// before the step kernel
 int prof_begin(lbm_ctx* c) {
     if (!c->profiling) return LBM_OK;
-    if (c->ev_used * 2 >= c->ev.size()) LBM_TRY(prof_drain(c));
-    return cuda_check(c, cudaEventRecord(c->ev[2 * c->ev_used], c->stream), "profile");
+    if (c->ev_used * 3 >= c->ev.size()) LBM_TRY(prof_drain(c));
+    return cuda_check(c, cudaEventRecord(c->ev[3 * c->ev_used], c->stream), "profile");
 }
+// after the step kernel
 int prof_end(lbm_ctx* c) {
     if (!c->profiling) return LBM_OK;
-    LBM_TRY(cuda_check(c, cudaEventRecord(c->ev[2 * c->ev_used + 1], c->stream), "profile"));
+    return cuda_check(c, cudaEventRecord(c->ev[3 * c->ev_used + 1], c->stream), "profile");
+}
+// after the step's boundary launches (none: right after prof_end)
+int prof_bound(lbm_ctx* c) {
+    if (!c->profiling) return LBM_OK;
+    LBM_TRY(cuda_check(c, cudaEventRecord(c->ev[3 * c->ev_used + 2], c->stream), "profile"));
     c->ev_used++;
     c->prof_launches++;
     return LBM_OK;
@@ -479,6 +490,7 @@ int step_one(lbm_ctx* c) {
     const SoaGrid& g = c->sg;
     dim3 grd((g.nx + 127) / 128, g.ny, g.nz);
     StepArgs a = step_args(c);
+    bool timed = false;   // a steady step of the general configuration (profile events open)
     if (c->state == ST_PRE) {
         S* b = (S*)c->buf[c->cur];
         k_step<Q, S, false, false><<<grd, 128, 0, c->stream>>>(b, b, a);
@@ -516,6 +528,7 @@ int step_one(lbm_ctx* c) {
                                          (const S*)c->buf[c->cur], a, nface), "folded boundaries"));
         c->launches++;
         LBM_LAUNCHED(c, "folded boundaries");
+        LBM_TRY(prof_bound(c));
         c->cur = nxt;
         c->it += 1;
         return LBM_OK;
@@ -533,6 +546,7 @@ int step_one(lbm_ctx* c) {
             LBM_LAUNCHED(c, "fused step");
         }
         LBM_TRY(prof_end(c));
+        timed = true;
         c->cur = nxt;
     }
     LBM_TRY(bc_state<Q, S>(c, c->cur, 1 - c->cur));
@@ -540,6 +554,7 @@ int step_one(lbm_ctx* c) {
     k_bump_step<<<1, 32, 0, c->stream>>>(c->d_it);
     c->launches++;
     LBM_LAUNCHED(c, "step counter");
+    if (timed) LBM_TRY(prof_bound(c));   // the boundaries of a timed step
     c->it += 1;
     return LBM_OK;
 }
@@ -1486,6 +1501,7 @@ int lbm_profile(lbm_ctx* c, int32_t enable) {
     LBM_TRY(prof_drain(c));
     c->profiling = enable != 0;
     c->prof_ms = 0.0;
+    c->prof_bc_ms = 0.0;
     c->prof_launches = 0;
     return LBM_OK;
 }
@@ -1495,6 +1511,14 @@ int lbm_profile_read(lbm_ctx* c, double* step_kernel_ms, int64_t* step_kernel_la
     LBM_TRY(prof_drain(c));
     *step_kernel_ms = c->prof_ms;
     *step_kernel_launches = c->prof_launches;
+    return LBM_OK;
+}
+
+int lbm_profile_read_boundary(lbm_ctx* c, double* boundary_ms, int64_t* steps) {
+    if (!c || !boundary_ms || !steps) return LBM_ERR_ARG;
+    LBM_TRY(prof_drain(c));
+    *boundary_ms = c->prof_bc_ms;
+    *steps = c->prof_launches;
     return LBM_OK;
 }
 

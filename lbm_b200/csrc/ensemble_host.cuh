@@ -12,8 +12,10 @@
 
 namespace {
 
-// launch shapes the autotuner chooses from: threads per block of k_ens_step
-constexpr int kEnsThreads[LBM_ENS_VARIANTS] = {64, 128, 256};
+// launch shapes the autotuner chooses from: threads per block of k_ens_step and
+// the minimum resident blocks per SM it is compiled for (its register cap)
+constexpr int kEnsThreads[LBM_ENS_VARIANTS] = {64, 64, 128, 128, 256, 256};
+constexpr int kEnsMinBlocks[LBM_ENS_VARIANTS] = {10, 12, 5, 6, 2, 3};
 
 // why the last lbm_ensemble_create of this thread failed (it returns no handle)
 thread_local std::string g_create_err;
@@ -29,9 +31,9 @@ struct lbm_ensemble {
     EnsMember* d_mem = nullptr;
     std::vector<EnsMember> h_mem;
     int2* d_blk = nullptr;           // per block (member, block within member): step grids per variant, then boundaries
-    size_t blk_off[LBM_ENS_VARIANTS + 1] = {0, 0, 0, 0};
-    int nblk[LBM_ENS_VARIANTS + 1] = {0, 0, 0, 0};
-    int variant = 1;
+    size_t blk_off[LBM_ENS_VARIANTS + 1] = {};
+    int nblk[LBM_ENS_VARIANTS + 1] = {};
+    int variant = 2;
     int graph_steps = LBM_ENS_GRAPH_STEPS;
     cudaGraphExec_t graph = nullptr;
     int graph_variant = -1;
@@ -96,10 +98,13 @@ int ens_launch_step(lbm_ensemble* e, int parity, cudaEvent_t* ev) {
     const EnsLayout Ls = ens_layout(e, e->variant);
     const int nb = e->nblk[e->variant];
     if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[0], e->stream), "ensemble profile"));
-    switch (kEnsThreads[e->variant]) {
-        case 64: k_ens_step<Q, S, 64, 10><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
-        case 128: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
-        default: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
+    switch (e->variant) {
+        case 0: k_ens_step<Q, S, 64, 10><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
+        case 1: k_ens_step<Q, S, 64, 12><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
+        case 2: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 3: k_ens_step<Q, S, 128, 6><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 4: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
+        default: k_ens_step<Q, S, 256, 3><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
     }
     LBM_TRY(echeck(e, cudaGetLastError(), "ensemble step"));
     if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[1], e->stream), "ensemble profile"));
@@ -357,6 +362,18 @@ int lbm_ensemble_profile(lbm_ensemble* e, int32_t nsteps, float* step_kernel_ms,
     return rc;
 }
 
+// mean ms per step of n steps launched as they would be by lbm_ensemble_step
+// (graph replay when allowed), timed with events on the ensemble's stream
+static int ens_time(lbm_ensemble* e, int n, bool graph, cudaEvent_t t0, cudaEvent_t t1, float* ms) {
+    LBM_TRY(echeck(e, cudaEventRecord(t0, e->stream), "autotune"));
+    LBM_TRY(ens_run(e, n, graph));
+    LBM_TRY(echeck(e, cudaEventRecord(t1, e->stream), "autotune"));
+    LBM_TRY(echeck(e, cudaEventSynchronize(t1), "autotune"));
+    LBM_TRY(echeck(e, cudaEventElapsedTime(ms, t0, t1), "autotune"));
+    *ms /= (float)n;
+    return LBM_OK;
+}
+
 int lbm_ensemble_autotune(lbm_ensemble* e, int32_t trial_steps, int32_t* variant, float* ms_per_step) {
     if (!e || trial_steps < 1) return LBM_ERR_ARG;
     int used = 0;
@@ -364,30 +381,56 @@ int lbm_ensemble_autotune(lbm_ensemble* e, int32_t trial_steps, int32_t* variant
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     LBM_TRY(echeck(e, cudaEventCreate(&t0), "cudaEventCreate"));
     int rc = echeck(e, cudaEventCreate(&t1), "cudaEventCreate");
+    // 1. every launch shape, direct launches: one warm-up step, then trial_steps timed
     float best = 0.f;
     int bestv = e->variant;
     for (int v = 0; v < LBM_ENS_VARIANTS && rc == LBM_OK; ++v) {
         e->variant = v;
-        rc = ens_run(e, 1, false);   // warm-up
-        if (rc == LBM_OK) rc = echeck(e, cudaEventRecord(t0, e->stream), "autotune");
-        if (rc == LBM_OK) rc = ens_run(e, trial_steps, false);
-        if (rc == LBM_OK) rc = echeck(e, cudaEventRecord(t1, e->stream), "autotune");
-        if (rc == LBM_OK) rc = echeck(e, cudaEventSynchronize(t1), "autotune");
         float ms = 0.f;
-        if (rc == LBM_OK) rc = echeck(e, cudaEventElapsedTime(&ms, t0, t1), "autotune");
+        rc = ens_run(e, 1, false);
+        if (rc == LBM_OK) rc = ens_time(e, trial_steps, false, t0, t1, &ms);
         if (rc != LBM_OK) break;
-        ms /= (float)trial_steps;
         if (ms_per_step) ms_per_step[v] = ms;
         if (v == 0 || ms < best) {
             best = ms;
             bestv = v;
         }
     }
+    e->variant = bestv;
+    // 2. the fastest shape replayed from graphs of LBM_ENS_GRAPH_STEPS steps against
+    // direct launches, over one graph's worth of steps each (graphs start on parity 0)
+    const int g = LBM_ENS_GRAPH_STEPS;
+    if (rc == LBM_OK && e->cur != 0) rc = ens_run(e, 1, false);
+    if (rc == LBM_OK) {
+        e->graph_steps = g;
+        rc = ens_run(e, g, true);   // capture and instantiate outside the timing
+    }
+    float ms_graph = 0.f, ms_direct = 0.f;
+    if (rc == LBM_OK) rc = ens_time(e, g, true, t0, t1, &ms_graph);
+    if (rc == LBM_OK) rc = ens_time(e, g, false, t0, t1, &ms_direct);
+    if (rc == LBM_OK && ms_direct < ms_graph) {
+        if (e->graph) cudaGraphExecDestroy(e->graph);
+        e->graph = nullptr;
+        e->graph_steps = 0;
+    }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
-    e->variant = bestv;
     if (variant) *variant = bestv;
     return rc;
+}
+
+int lbm_ensemble_get_config(const lbm_ensemble* e, int32_t* variant, int32_t* graph_steps) {
+    if (!e) return LBM_ERR_ARG;
+    if (variant) *variant = e->variant;
+    if (graph_steps) *graph_steps = e->graph_steps;
+    return LBM_OK;
+}
+
+int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks) {
+    if (variant < 0 || variant >= LBM_ENS_VARIANTS) return LBM_ERR_ARG;
+    if (threads) *threads = kEnsThreads[variant];
+    if (min_blocks) *min_blocks = kEnsMinBlocks[variant];
+    return LBM_OK;
 }
 
 }  // extern "C"

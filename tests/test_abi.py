@@ -88,7 +88,7 @@ def test_null_context_is_an_error_not_a_crash(lib):
     """Every entry point that takes a context (or an ensemble) as its first
     argument answers LBM_ERR_ARG to a null one, before touching the GPU."""
     no_context = {"lbm_create", "lbm_abi_version", "lbm_last_error", "lbm_ensemble_last_error",
-                  "lbm_ensemble_create", "lbm_mass_momentum_noalloc"}
+                  "lbm_ensemble_create", "lbm_mass_momentum_noalloc", "lbm_ensemble_variant_shape"}
     checked = 0
     for name in header_functions():
         if name in no_context:
@@ -104,6 +104,20 @@ def test_null_context_is_an_error_not_a_crash(lib):
         assert getattr(lib, name)(*args) == _lib.LBM_ERR_ARG, name
         checked += 1
     assert checked >= 70
+
+
+def test_ensemble_launch_shapes(lib):
+    """The autotuner's launch shapes: distinct (threads, min blocks per SM) pairs
+    whose register caps the compiler can meet, out-of-range variants refused."""
+    t, m = ctypes.c_int32(0), ctypes.c_int32(0)
+    shapes = []
+    for v in range(_lib.LBM_ENS_VARIANTS):
+        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m)) == _lib.LBM_OK
+        assert t.value in (64, 128, 256) and 1 <= m.value and t.value * m.value <= 2048
+        shapes.append((t.value, m.value))
+    assert len(set(shapes)) == len(shapes)
+    for v in (-1, _lib.LBM_ENS_VARIANTS):
+        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m)) == _lib.LBM_ERR_ARG
 
 
 def test_create_rejects_bad_params_before_touching_the_gpu(lib):

@@ -57,9 +57,13 @@ def test_members_match_single_runs(storage, graph):
 
 
 def test_every_launch_shape_and_autotune():
+    from lbm_b200 import Ensemble, _lib
     from lbm_b200.ensemble import build_ensemble
+    V, G = _lib.LBM_ENS_VARIANTS, _lib.LBM_ENS_GRAPH_STEPS
+    shapes = [Ensemble.variant_shape(v) for v in range(V)]
+    assert len(set(shapes)) == V and all(t in (64, 128, 256) and m >= 1 for t, m in shapes)
     ref = [alone(wl, 9) for wl in MEMBERS]
-    for v in range(3):
+    for v in range(V):
         ens = build_ensemble(MEMBERS)
         ens.set_variant(v)
         ens.step(9)
@@ -68,9 +72,21 @@ def test_every_launch_shape_and_autotune():
         ens.close()
     ens = build_ensemble(MEMBERS)
     v, ms = ens.autotune(2)
-    assert 0 <= v < 3 and all(t > 0 for t in ms) and ms[v] == min(ms)
+    assert 0 <= v < V and all(t > 0 for t in ms) and ms[v] == min(ms)
+    cv, cg = ens.config()
+    assert cv == v and cg in (0, G)
     ens.step(4)
-    assert all(L.it == 1 + 3 * (2 + 1) + 4 for L in ens.members)   # first step, 3 x (warm-up + 2), 4
+    # the first step (collides in place: the buffer parity stays), V x (warm-up + 2), one step
+    # back to parity 0 where needed, graph capture + 2 timed graphs' worth, then 4
+    n = V * 3
+    assert all(L.it == 1 + n + n % 2 + 3 * G + 4 for L in ens.members)
+    ens.close()
+    ref = [alone(wl, 8) for wl in MEMBERS]
+    ens = build_ensemble(MEMBERS)
+    ens.set_graph(4)      # graph replay: same results as direct launches
+    ens.step(8)
+    for m, got in enumerate(exported(ens)):
+        assert all(np.array_equal(a, b) for a, b in zip(got, ref[m])), m
     ens.close()
 
 
