@@ -499,6 +499,7 @@ def ensemble_measure(a, members, dist=None):
             "roofline": {"bound": "hbm", "achieved": round(cells * bl / (k_step * 1e-3) / 1e9, 1), "peak": hbm,
                          "unit": "GB/s", "frac": round(cells * bl / (k_step * 1e-3) / 1e9 / hbm, 4),
                          "peak_kind": hbm_kind, "kernel": "k_ens_step<19,float>", "kernel_ms": round(k_step, 4),
+                         "traffic": ncu_traffic("k_ens_step<19,float>", cells),
                          "boundary_kernel_ms": round(k_bc, 4),
                          "step_frac": round(cells * bl / (ms / a.steps * 1e-3) / 1e9 / hbm, 4),
                          "note": "frac: the step kernel alone (CUDA events around each launch, %d direct-launch "
@@ -970,6 +971,7 @@ def main():
         line["f16_storage"] = {"value": round(v16, 1), "unit": "MLUPS", "speedup_vs_f32": round(v16 / value, 3),
                                "roofline_frac": round(ach16 / hbm, 4) if ach16 else None,
                                "kernel_ms": round(kms16 / max(kn16, 1), 4),
+                               "traffic": ncu_traffic("k_step_pair<%d,__half>" % wl.nl, cells),
                                "boundary_kernel_ms": round(bms16 / max(kn16, 1), 4),
                                "ms_per_step": round(ms16 / a.steps, 4)}
         torch.cuda.empty_cache()
