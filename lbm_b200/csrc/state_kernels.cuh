@@ -168,9 +168,9 @@ __device__ __forceinline__ void store_sector(S* p, S v, int slot) {
 
 // The inflow ghost value of a direction whose source is the post-collision
 // value fin of direction ls (weight wl, velocity (cx, cy)) at the cell i = 1,
-// with uu the inflow speed of the cell's k (m_boundary_i_inflow_kernel.F90:
-// 56-111): fin - 2 wl rho0 (cx uu cos + cy uu sin) / cs2, rounded operation by
-// operation in that order.
+// with uu the inflow speed of the cell's k
+// (m_boundary_i_inflow_kernel.F90:56-111): fin - 2 wl rho0 (cx uu cos + cy uu
+// sin) / cs2, rounded operation by operation in that order.
 __device__ __forceinline__ float inflow_value(float fin, float wl, int cx, int cy, float uu, const StepArgs& a) {
     const float t = __fadd_rn(__fmul_rn(__fmul_rn((float)cx, uu), a.cosd), __fmul_rn(__fmul_rn((float)cy, uu), a.sind));
     const float p = __fmul_rn(__fmul_rn(__fmul_rn(2.0f, wl), a.rho0), t);
@@ -187,7 +187,7 @@ __device__ __forceinline__ float inflow_value(float fin, float wl, int cx, int c
 //     source is an interior cell, and f1(m,i,j,kg) = f2(l,i,j,kg) for the
 //     reflected direction m (m_boundary_k_closed_kernel.F90:35-46).
 //   * x-ghost threads: the inflow ghost (0,j,k) and the outflow ghost
-//     (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:184-231), written to the
+//     (nx+1,j,k) (m_boundary_i_inflow_kernel.F90:56-111), written to the
 //     compact x-ghost array, and into the rows for the directions the next pull
 //     reads there (cx > 0 at i = 0, cx < 0 at nx+1).  At the planes k=1 and
 //     k=nz they first pass the value those row ghosts held before this step to
