@@ -416,13 +416,26 @@ __device__ __forceinline__ void pair_update(f2 (&fp)[Q], S* __restrict__ dst, co
                                             int j, int k) {
     pair_collide<Q, S, FORCE>(fp, a, i, j, k);
     S* q = dst + o;
+    if constexpr (sizeof(S) == 2) {
+        // the edge copy reuses the stored half2 values (no second conversion)
+        __half2 h[Q];
 #pragma unroll
-    for (int l = 0; l < Q; ++l) {
-        char* qb = reinterpret_cast<char*>(q) + a.soffb[l];
-        if constexpr (sizeof(S) == 2) *reinterpret_cast<__half2*>(qb) = __floats2half2_rn(fp[l].x, fp[l].y);
-        else *reinterpret_cast<float2*>(qb) = fp[l];
+        for (int l = 0; l < Q; ++l) {
+            h[l] = __floats2half2_rn(fp[l].x, fp[l].y);
+            *reinterpret_cast<__half2*>(reinterpret_cast<char*>(q) + a.soffb[l]) = h[l];
+        }
+        if (FOLD && (i == 1 || i + 1 == a.g.nx)) {
+            const long long nyz = (long long)a.g.ny * a.g.nz;
+            const int c = (i == 1) ? 0 : 1;
+            __half* e = (__half*)a.edge + (long long)c * Q * nyz + (long long)(k - 1) * a.g.ny + (j - 1);
+#pragma unroll
+            for (int l = 0; l < Q; ++l) e[l * nyz] = c ? __high2half(h[l]) : __low2half(h[l]);
+        }
+    } else {
+#pragma unroll
+        for (int l = 0; l < Q; ++l) *reinterpret_cast<float2*>(reinterpret_cast<char*>(q) + a.soffb[l]) = fp[l];
+        if (FOLD) pair_edge<Q, S>(fp, a, i, j, k);
     }
-    if (FOLD) pair_edge<Q, S>(fp, a, i, j, k);
 }
 
 // One pair (i, i+1), i odd, of row (j, k): pull, collide, store.  WRAP: periodic
