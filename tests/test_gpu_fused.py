@@ -221,6 +221,35 @@ def test_status_flags_bad_density():
     assert L.status() == 0          # cleared by the read
 
 
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+def test_status_flags_nan_in_the_pair_step(storage):
+    """A NaN population spreads through the steady steps of the two-cells-per-
+    thread kernel, which must raise the flag on every step it is seen."""
+    from lbm_b200 import Lbm
+    wl = SMALL.with_(sphere=None, lturb=False)
+    L = Lbm(params_of(wl, storage=storage))
+    L.set_kernel("pair")
+    rho, u, v, w = (cuda(a) for a in W.initial_macro(wl))
+    feq = L.empty_f()
+    L.fequil3(feq, rho, u, v, w)
+    L.fillghosts(feq)
+    f2 = feq.clone()
+    L.state_import(feq, f2, rho, u, v, w)
+    L.set_inflow(cuda(W.inflow_profile(wl)))
+    L.step(2)
+    assert L.status() == 0
+    f1, f2 = L.empty_f(), L.empty_f()
+    L.state_export(f1, f2)
+    f1[4, 5, 6, 7] = float("nan")   # one population of one interior cell (reference layout: k, j, i, l)
+    L.get_macro(rho, u, v, w)
+    L.state_import(f1, f2, rho, u, v, w)
+    L.step(1)                       # the in-place first step after the import
+    L.status()
+    for _ in range(2):
+        L.step(1)                   # steady steps: the pair kernel
+        assert L.status() & 1
+
+
 def test_sphere_200_steps_parity():
     """128x64x64 D3Q27, sphere r=8, 200 steps: rel L2 <= 1e-5 vs the FP32 oracle."""
     wl = W.SPHERE_128
