@@ -464,7 +464,11 @@ cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream
 // state size (64-bit byte offsets)
 bool pair_shape_ok(const lbm_ctx* c) { return c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
 bool pair_ok(const lbm_ctx* c) { return c->kernel == LBM_KERNEL_PAIR && pair_shape_ok(c); }
-dim3 pair_grid(const lbm_ctx* c) { return dim3((unsigned)((c->p.nx / 2 + 127) / 128), c->p.ny, c->p.nz); }
+template <int Q, typename S>
+dim3 pair_grid(const lbm_ctx* c) {
+    constexpr int t = pair_threads<Q, S>();
+    return dim3((unsigned)((c->p.nx / 2 + t - 1) / t), c->p.ny, c->p.nz);
+}
 
 // the steady step from buffer cur into nxt, two cells per thread
 template <int Q, typename S, bool WRAP, bool FOLD>
@@ -472,11 +476,11 @@ int pair_family_step(lbm_ctx* c, int nxt, const StepArgs& a) {
     const S* src = (const S*)c->buf[c->cur];
     S* dst = (S*)c->buf[nxt];
     if (c->force)
-        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, true, FOLD>, pair_grid(c), dim3(128), c->stream, src, dst, a),
-                           "fused step (pair)"));
+        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, true, FOLD>, pair_grid<Q, S>(c),
+                                         dim3(pair_threads<Q, S>()), c->stream, src, dst, a), "fused step (pair)"));
     else
-        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, false, FOLD>, pair_grid(c), dim3(128), c->stream, src, dst,
-                                         a), "fused step (pair)"));
+        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, false, FOLD>, pair_grid<Q, S>(c),
+                                         dim3(pair_threads<Q, S>()), c->stream, src, dst, a), "fused step (pair)"));
     c->launches++;
     LBM_LAUNCHED(c, "fused step (pair)");
     return LBM_OK;
