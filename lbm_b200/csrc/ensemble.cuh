@@ -32,11 +32,13 @@ struct EnsLayout {
     const int2* blk;     // per block of this launch's grid: (member, block index within the member)
 };
 
-// the member's arguments into shared memory (word copy; StepArgs is 8-byte aligned)
+// the member's arguments into shared memory, in 16-byte words (StepArgs is
+// 16-byte aligned: one load per thread for blocks of 64 threads or more)
 __device__ __forceinline__ void ens_load_args(unsigned char* raw, const StepArgs* ga) {
-    constexpr int n = (int)(sizeof(StepArgs) / 4);
+    static_assert(sizeof(StepArgs) % 16 == 0, "StepArgs is copied in 16-byte words");
+    constexpr int n = (int)(sizeof(StepArgs) / 16);
     for (int w = threadIdx.x; w < n; w += blockDim.x)
-        reinterpret_cast<int*>(raw)[w] = __ldg(reinterpret_cast<const int*>(ga) + w);
+        reinterpret_cast<uint4*>(raw)[w] = __ldg(reinterpret_cast<const uint4*>(ga) + w);
     __syncthreads();
 }
 

@@ -49,7 +49,8 @@ __device__ __forceinline__ unsigned fdiv(unsigned n, const FastDiv& f) {
     return f.d == 1u ? n : (__umulhi(n, f.m) >> f.s);
 }
 
-struct StepArgs {
+// 16-byte aligned: the ensemble kernels copy it into shared memory in 16-byte words
+struct alignas(16) StepArgs {
     SoaGrid g;
     CollideParams cp;
     const uint8_t* solid;     // interior mask [k-1][j-1][i-1], or null
