@@ -488,9 +488,9 @@ def ensemble_measure(a, members, dist=None):
                         "autotune": {"variant": variant, "shape": Ensemble.variant_shape(variant),
                                      "shapes": [Ensemble.variant_shape(v) for v in range(_lib.LBM_ENS_VARIANTS)],
                                      "shape_ms_per_step": [round(x, 4) for x in vms],
-                                     "how": "each (threads per block, min blocks per SM) shape over 5 direct-launch "
-                                            "steps, then the fastest replayed from %d-step graphs vs launched "
-                                            "directly" % _lib.LBM_ENS_GRAPH_STEPS}},
+                                     "how": "each (threads per block, min blocks per SM, tiles per block) shape "
+                                            "over 5 direct-launch steps, then the fastest replayed from %d-step "
+                                            "graphs vs launched directly" % _lib.LBM_ENS_GRAPH_STEPS}},
             ("direct_launches" if graph_steps else "graph_replay"):
                 {"value": round(mlups(ms_other), 1), "ms_per_step": round(ms_other / a.steps, 4)},
             "sequential": {"value": round(mlups(ms_seq), 1), "ms_per_step": round(ms_seq / a.steps, 4),

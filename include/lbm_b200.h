@@ -371,7 +371,7 @@ int lbm_state_adjoint_export(lbm_ctx* ctx, float* fhat, const float* A);
  * nx >= 4, and one lattice and storage for all. */
 typedef struct lbm_ensemble lbm_ensemble;
 enum {
-    LBM_ENS_VARIANTS = 6,      /* launch shapes of the step kernel: lbm_ensemble_variant_shape   */
+    LBM_ENS_VARIANTS = 8,      /* launch shapes of the step kernel: lbm_ensemble_variant_shape   */
     LBM_ENS_GRAPH_STEPS = 16   /* steps per captured graph (default; lbm_ensemble_set_graph)       */
 };
 int lbm_ensemble_create(lbm_ensemble** ens, const lbm_params* members, int32_t nmembers);
@@ -398,9 +398,10 @@ int lbm_ensemble_autotune(lbm_ensemble* ens, int32_t trial_steps, int32_t* varia
 int lbm_ensemble_set_variant(lbm_ensemble* ens, int32_t variant);
 /* the launch shape and graph steps in use (either pointer may be NULL) */
 int lbm_ensemble_get_config(const lbm_ensemble* ens, int32_t* variant, int32_t* graph_steps);
-/* launch shape `variant` of the step kernel: threads per block and the minimum
- * resident blocks per SM it is compiled for (which caps its registers) */
-int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks);
+/* launch shape `variant` of the step kernel: threads per block, the minimum
+ * resident blocks per SM it is compiled for (which caps its registers) and the
+ * tiles of `threads` pairs each block covers (any pointer may be NULL) */
+int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks, int32_t* tiles);
 /* advance nsteps batched steps with direct launches (no graph), timing every
  * launch with CUDA events; returns the mean duration of the step kernel and of
  * the boundary kernel in ms.  Synchronises the ensemble's stream. */

@@ -388,11 +388,11 @@ module lbm_b200_iface
          type(c_ptr), value        :: ens
          integer(c_int32_t)        :: variant, graph_steps
       end function
-      integer(c_int) function lbm_ensemble_variant_shape(variant, threads, min_blocks) &
+      integer(c_int) function lbm_ensemble_variant_shape(variant, threads, min_blocks, tiles) &
             bind(C, name="lbm_ensemble_variant_shape")
          import :: c_int, c_int32_t
          integer(c_int32_t), value :: variant
-         integer(c_int32_t)        :: threads, min_blocks
+         integer(c_int32_t)        :: threads, min_blocks, tiles
       end function
       integer(c_int) function lbm_ensemble_set_graph(ens, graph_steps) bind(C, name="lbm_ensemble_set_graph")
          import :: c_ptr, c_int, c_int32_t

@@ -27,7 +27,7 @@ LBM_STATUS_BAD_DENSITY = 1
 LBM_STATUS_TIMEOUT = 4
 LBM_KERNEL_PULL = 1
 LBM_KERNEL_PAIR = 2
-LBM_ENS_VARIANTS = 6
+LBM_ENS_VARIANTS = 8
 LBM_ENS_GRAPH_STEPS = 16
 
 
@@ -130,7 +130,8 @@ SIGNATURES = {
     "lbm_ensemble_autotune": [P, I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_variant": [P, I],
     "lbm_ensemble_get_config": [P, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
-    "lbm_ensemble_variant_shape": [I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+    "lbm_ensemble_variant_shape": [I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_int32)],
     "lbm_ensemble_profile": [P, I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)],
     "lbm_ensemble_set_graph": [P, I],
 }

@@ -503,13 +503,14 @@ class Ensemble:
 
     @staticmethod
     def variant_shape(variant: int):
-        """(threads per block, minimum resident blocks per SM) of a launch shape."""
+        """(threads per block, minimum resident blocks per SM, tiles per block) of
+        a launch shape."""
         L = _lib.load()
-        t, m = ctypes.c_int32(0), ctypes.c_int32(0)
-        rc = L.lbm_ensemble_variant_shape(int(variant), ctypes.byref(t), ctypes.byref(m))
+        t, m, r = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+        rc = L.lbm_ensemble_variant_shape(int(variant), ctypes.byref(t), ctypes.byref(m), ctypes.byref(r))
         if rc != 0:
             raise LbmError(rc, "variant %d out of range" % variant)
-        return t.value, m.value
+        return t.value, m.value, r.value
 
     def set_variant(self, v: int):
         self._call("lbm_ensemble_set_variant", int(v))

@@ -11,9 +11,11 @@
 // per-pair (pair_cell) or per-block (bc_fold_block) code as the single-state
 // kernels, so a member of an ensemble computes exactly what it computes alone.
 //
-// In k_ens_step a block of T threads covers T consecutive pairs of the
-// member's pairs flattened row by row (pair q: i = 2 (q mod nx/2) + 1, row
-// q div nx/2), so rows shorter than a block leave no threads idle.
+// In k_ens_step a block of T threads covers R consecutive tiles of T
+// consecutive pairs of the member's pairs flattened row by row (pair q:
+// i = 2 (q mod nx/2) + 1, row q div nx/2), so rows shorter than a block leave
+// no threads idle, and a block's set-up (its table entry and the member's
+// arguments) serves R tiles.
 #pragma once
 
 #include "pair_step.cuh"
@@ -42,7 +44,7 @@ __device__ __forceinline__ void ens_load_args(unsigned char* raw, const StepArgs
     __syncthreads();
 }
 
-template <int Q, typename S, int T, int MINB>
+template <int Q, typename S, int T, int MINB, int R>
 __global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
     __shared__ __align__(16) unsigned char raw[sizeof(StepArgs)];
     const int2 mb = __ldg(L.blk + blockIdx.x);
@@ -51,16 +53,19 @@ __global__ void __launch_bounds__(T, MINB) k_ens_step(EnsLayout L, int parity) {
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
     // 32-bit decode by multiply-high (a member holds fewer than 2^31 pairs)
     const unsigned hp = (unsigned)(a.g.nx / 2);
-    const unsigned q = (unsigned)mb.y * T + threadIdx.x;
-    if (q >= hp * (unsigned)a.g.ny * (unsigned)a.g.nz) return;
-    const unsigned row = fdiv(q, em->hp);
-    const int i = 2 * (int)(q - row * hp) + 1;
-    const unsigned kk = fdiv(row, em->ny);
-    const int j = (int)(row - kk * (unsigned)a.g.ny) + 1;
-    const int k = (int)kk + 1;
+    const unsigned npairs = hp * (unsigned)a.g.ny * (unsigned)a.g.nz;
     const S* src = reinterpret_cast<const S*>(em->buf[parity]);
     S* dst = reinterpret_cast<S*>(em->buf[1 - parity]);
-    pair_cell<Q, S, true>(src, dst, a, i, j, k);
+    for (int r = 0; r < R; ++r) {
+        const unsigned q = ((unsigned)mb.y * R + r) * T + threadIdx.x;
+        if (q >= npairs) return;   // the later tiles are past the member's end too
+        const unsigned row = fdiv(q, em->hp);
+        const int i = 2 * (int)(q - row * hp) + 1;
+        const unsigned kk = fdiv(row, em->ny);
+        const int j = (int)(row - kk * (unsigned)a.g.ny) + 1;
+        const int k = (int)kk + 1;
+        pair_cell<Q, S, true>(src, dst, a, i, j, k);
+    }
 }
 
 template <int Q, typename S>

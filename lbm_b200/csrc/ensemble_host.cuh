@@ -12,10 +12,12 @@
 
 namespace {
 
-// launch shapes the autotuner chooses from: threads per block of k_ens_step and
-// the minimum resident blocks per SM it is compiled for (its register cap)
-constexpr int kEnsThreads[LBM_ENS_VARIANTS] = {64, 64, 128, 128, 256, 256};
-constexpr int kEnsMinBlocks[LBM_ENS_VARIANTS] = {10, 12, 5, 6, 2, 3};
+// launch shapes the autotuner chooses from: threads per block of k_ens_step,
+// the minimum resident blocks per SM it is compiled for (its register cap) and
+// the tiles of a block's threads each block covers
+constexpr int kEnsThreads[LBM_ENS_VARIANTS] = {64, 64, 128, 128, 128, 128, 256, 256};
+constexpr int kEnsMinBlocks[LBM_ENS_VARIANTS] = {12, 12, 5, 6, 5, 6, 3, 3};
+constexpr int kEnsTiles[LBM_ENS_VARIANTS] = {1, 2, 2, 2, 4, 4, 2, 4};
 
 // why the last lbm_ensemble_create of this thread failed (it returns no handle)
 thread_local std::string g_create_err;
@@ -33,7 +35,7 @@ struct lbm_ensemble {
     int2* d_blk = nullptr;           // per block (member, block within member): step grids per variant, then boundaries
     size_t blk_off[LBM_ENS_VARIANTS + 1] = {};
     int nblk[LBM_ENS_VARIANTS + 1] = {};
-    int variant = 2;
+    int variant = 3;
     int graph_steps = LBM_ENS_GRAPH_STEPS;
     cudaGraphExec_t graph = nullptr;
     int graph_variant = -1;
@@ -99,12 +101,14 @@ int ens_launch_step(lbm_ensemble* e, int parity, cudaEvent_t* ev) {
     const int nb = e->nblk[e->variant];
     if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[0], e->stream), "ensemble profile"));
     switch (e->variant) {
-        case 0: k_ens_step<Q, S, 64, 10><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
-        case 1: k_ens_step<Q, S, 64, 12><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
-        case 2: k_ens_step<Q, S, 128, 5><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
-        case 3: k_ens_step<Q, S, 128, 6><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
-        case 4: k_ens_step<Q, S, 256, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
-        default: k_ens_step<Q, S, 256, 3><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
+        case 0: k_ens_step<Q, S, 64, 12, 1><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
+        case 1: k_ens_step<Q, S, 64, 12, 2><<<nb, 64, 0, e->stream>>>(Ls, parity); break;
+        case 2: k_ens_step<Q, S, 128, 5, 2><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 3: k_ens_step<Q, S, 128, 6, 2><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 4: k_ens_step<Q, S, 128, 5, 4><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 5: k_ens_step<Q, S, 128, 6, 4><<<nb, 128, 0, e->stream>>>(Ls, parity); break;
+        case 6: k_ens_step<Q, S, 256, 3, 2><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
+        default: k_ens_step<Q, S, 256, 3, 4><<<nb, 256, 0, e->stream>>>(Ls, parity); break;
     }
     LBM_TRY(echeck(e, cudaGetLastError(), "ensemble step"));
     if (ev) LBM_TRY(echeck(e, cudaEventRecord(ev[1], e->stream), "ensemble profile"));
@@ -250,7 +254,8 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
                 if (v < LBM_ENS_VARIANTS) {
                     const long long pairs = (long long)(g.nx / 2) * g.ny * g.nz;
                     if (pairs >= (1LL << 31)) rc = efail(e, LBM_ERR_UNSUPPORTED, "member %d: 2^31 pairs or more", (int)k);
-                    nb = (pairs + kEnsThreads[v] - 1) / kEnsThreads[v];
+                    const long long per_block = (long long)kEnsThreads[v] * kEnsTiles[v];
+                    nb = (pairs + per_block - 1) / per_block;
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
                     nb = bc_fold_face_blocks(g) + bc_fold_xg_blocks(g, e->nl, true);
@@ -426,10 +431,11 @@ int lbm_ensemble_get_config(const lbm_ensemble* e, int32_t* variant, int32_t* gr
     return LBM_OK;
 }
 
-int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks) {
+int lbm_ensemble_variant_shape(int32_t variant, int32_t* threads, int32_t* min_blocks, int32_t* tiles) {
     if (variant < 0 || variant >= LBM_ENS_VARIANTS) return LBM_ERR_ARG;
     if (threads) *threads = kEnsThreads[variant];
     if (min_blocks) *min_blocks = kEnsMinBlocks[variant];
+    if (tiles) *tiles = kEnsTiles[variant];
     return LBM_OK;
 }
 

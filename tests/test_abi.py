@@ -107,17 +107,18 @@ def test_null_context_is_an_error_not_a_crash(lib):
 
 
 def test_ensemble_launch_shapes(lib):
-    """The autotuner's launch shapes: distinct (threads, min blocks per SM) pairs
-    whose register caps the compiler can meet, out-of-range variants refused."""
-    t, m = ctypes.c_int32(0), ctypes.c_int32(0)
+    """The autotuner's launch shapes: distinct (threads, min blocks per SM, tiles
+    per block) whose register caps the compiler can meet, out-of-range variants
+    refused."""
+    t, m, r = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
     shapes = []
     for v in range(_lib.LBM_ENS_VARIANTS):
-        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m)) == _lib.LBM_OK
-        assert t.value in (64, 128, 256) and 1 <= m.value and t.value * m.value <= 2048
-        shapes.append((t.value, m.value))
+        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m), ctypes.byref(r)) == _lib.LBM_OK
+        assert t.value in (64, 128, 256) and 1 <= m.value and t.value * m.value <= 2048 and r.value in (1, 2, 4)
+        shapes.append((t.value, m.value, r.value))
     assert len(set(shapes)) == len(shapes)
     for v in (-1, _lib.LBM_ENS_VARIANTS):
-        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m)) == _lib.LBM_ERR_ARG
+        assert lib.lbm_ensemble_variant_shape(v, ctypes.byref(t), ctypes.byref(m), ctypes.byref(r)) == _lib.LBM_ERR_ARG
 
 
 def test_create_rejects_bad_params_before_touching_the_gpu(lib):

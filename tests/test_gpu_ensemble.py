@@ -61,7 +61,7 @@ def test_every_launch_shape_and_autotune():
     from lbm_b200.ensemble import build_ensemble
     V, G = _lib.LBM_ENS_VARIANTS, _lib.LBM_ENS_GRAPH_STEPS
     shapes = [Ensemble.variant_shape(v) for v in range(V)]
-    assert len(set(shapes)) == V and all(t in (64, 128, 256) and m >= 1 for t, m in shapes)
+    assert len(set(shapes)) == V and all(t in (64, 128, 256) and m >= 1 and r >= 1 for t, m, r in shapes)
     ref = [alone(wl, 9) for wl in MEMBERS]
     for v in range(V):
         ens = build_ensemble(MEMBERS)
