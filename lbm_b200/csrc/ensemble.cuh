@@ -76,7 +76,7 @@ __global__ void __launch_bounds__(128) k_ens_bc(EnsLayout L, int parity) {
     ens_load_args(raw, &em->a[parity]);
     const StepArgs& a = *reinterpret_cast<const StepArgs*>(raw);
     bc_fold_block<Q, S, true>(reinterpret_cast<S*>(em->buf[1 - parity]), reinterpret_cast<const S*>(em->buf[parity]), a,
-                        em->nface_blocks, mb.y);
+                              em->nface_blocks, mb.y);
 }
 
 }  // namespace lbm

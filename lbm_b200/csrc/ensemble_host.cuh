@@ -85,7 +85,7 @@ int ens_upload(lbm_ensemble* e) {
         c->cur = keep;
         d.buf[0] = c->buf[0];
         d.buf[1] = c->buf[1];
-        d.nface_blocks = bc_fold_face_blocks(c->sg);
+        d.nface_blocks = bc_fold_face_blocks(c->sg, true);
         d.hp = make_fastdiv((unsigned)(c->sg.nx / 2));
         d.ny = make_fastdiv((unsigned)c->sg.ny);
     }
@@ -258,7 +258,7 @@ int lbm_ensemble_create(lbm_ensemble** out, const lbm_params* members, int32_t n
                     nb = (pairs + per_block - 1) / per_block;
                 } else {
                     // k_bc_fold's grid: k-face blocks, then x-ghost blocks
-                    nb = bc_fold_face_blocks(g) + bc_fold_xg_blocks(g, e->nl, true);
+                    nb = bc_fold_face_blocks(g, true) + bc_fold_xg_blocks(g, e->nl, true);
                 }
                 for (long long b = 0; b < nb; ++b) blk.push_back(make_int2((int)k, (int)b));
             }

@@ -339,12 +339,24 @@ template <int Q, typename S, bool WIDE>
 __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs& a, int nface_blocks, int vb) {
     const SoaGrid& g = a.g;
     if (vb < nface_blocks) {
-        const int per_row = (g.nx + 127) / 128;
-        const int b = vb;
-        const int side = b / (per_row * g.ny);
-        const int j = (b / per_row) % g.ny + 1;
-        const int i = (b % per_row) * 128 + threadIdx.x + 1;
-        if (i > g.nx) return;
+        int side, i, j;
+        if (WIDE) {
+            // (i, j, face) flattened, i fastest: no idle threads for rows shorter than a block
+            const long long e = (long long)vb * 128 + threadIdx.x;
+            const long long nxy = (long long)g.nx * g.ny;
+            if (e >= 2 * nxy) return;
+            side = e >= nxy ? 1 : 0;
+            const long long r = e - side * nxy;
+            j = (int)(r / g.nx) + 1;
+            i = (int)(r - (long long)(j - 1) * g.nx) + 1;
+        } else {
+            const int per_row = (g.nx + 127) / 128;
+            const int b = vb;
+            side = b / (per_row * g.ny);
+            j = (b / per_row) % g.ny + 1;
+            i = (b % per_row) * 128 + threadIdx.x + 1;
+            if (i > g.nx) return;
+        }
         if (side) bc_fold_face<Q, S, 1>(f1, f2, g, a.kopt_hi, i, j);
         else bc_fold_face<Q, S, 0>(f1, f2, g, a.kopt_lo, i, j);
         return;
@@ -366,8 +378,11 @@ __device__ __forceinline__ void bc_fold_block(S* f1, const S* f2, const StepArgs
     else bc_fold_xcol<Q, S, 0>(f1, a, j, k, cell);
 }
 
-// blocks of bc_fold_block: the k-face blocks, then the x-ghost blocks
-__host__ __device__ inline int bc_fold_face_blocks(const SoaGrid& g) { return 2 * g.ny * ((g.nx + 127) / 128); }
+// blocks of bc_fold_block: the k-face blocks, then the x-ghost blocks (WIDE:
+// the ensemble's layout, k-face threads flattened over (i, j, face))
+__host__ __device__ inline int bc_fold_face_blocks(const SoaGrid& g, bool wide = false) {
+    return wide ? (int)((2LL * g.nx * g.ny + 127) / 128) : 2 * g.ny * ((g.nx + 127) / 128);
+}
 __host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q, bool wide) {
     return ((wide ? 2LL : (long long)Q) * g.ny * g.nz + 127) / 128;
 }
