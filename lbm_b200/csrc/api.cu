@@ -464,10 +464,11 @@ cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream
 // state size (64-bit byte offsets)
 bool pair_shape_ok(const lbm_ctx* c) { return c->p.ihrr == 1 && c->p.nx % 2 == 0 && c->p.nx >= 4; }
 bool pair_ok(const lbm_ctx* c) { return c->kernel == LBM_KERNEL_PAIR && pair_shape_ok(c); }
-template <int Q, typename S>
-dim3 pair_grid(const lbm_ctx* c) {
-    constexpr int t = pair_threads<Q, S>();
-    return dim3((unsigned)((c->p.nx / 2 + t - 1) / t), c->p.ny, c->p.nz);
+dim3 pair_grid(const lbm_ctx* c, int t) { return dim3((unsigned)((c->p.nx / 2 + t - 1) / t), c->p.ny, c->p.nz); }
+
+template <int Q, typename S, bool WRAP, bool FORCE, bool FOLD, int T>
+cudaError_t pair_launch(lbm_ctx* c, const S* src, S* dst, const StepArgs& a) {
+    return launch_pdl(k_step_pair<Q, S, WRAP, FORCE, FOLD, T>, pair_grid(c, T), dim3(T), c->stream, src, dst, a);
 }
 
 // the steady step from buffer cur into nxt, two cells per thread
@@ -475,12 +476,16 @@ template <int Q, typename S, bool WRAP, bool FOLD>
 int pair_family_step(lbm_ctx* c, int nxt, const StepArgs& a) {
     const S* src = (const S*)c->buf[c->cur];
     S* dst = (S*)c->buf[nxt];
+    // blocks of 256 threads where that shape is compiled and a row's pairs fill them
+    const bool wide = pair_wide_ok<Q, S>() && (c->p.nx / 2) % 256 == 0;
+    cudaError_t r;
     if (c->force)
-        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, true, FOLD>, pair_grid<Q, S>(c),
-                                         dim3(pair_threads<Q, S>()), c->stream, src, dst, a), "fused step (pair)"));
+        r = wide ? pair_launch<Q, S, WRAP, true, FOLD, pair_wide_ok<Q, S>() ? 256 : 128>(c, src, dst, a)
+                 : pair_launch<Q, S, WRAP, true, FOLD, 128>(c, src, dst, a);
     else
-        LBM_TRY(cuda_check(c, launch_pdl(k_step_pair<Q, S, WRAP, false, FOLD>, pair_grid<Q, S>(c),
-                                         dim3(pair_threads<Q, S>()), c->stream, src, dst, a), "fused step (pair)"));
+        r = wide ? pair_launch<Q, S, WRAP, false, FOLD, pair_wide_ok<Q, S>() ? 256 : 128>(c, src, dst, a)
+                 : pair_launch<Q, S, WRAP, false, FOLD, 128>(c, src, dst, a);
+    LBM_TRY(cuda_check(c, r, "fused step (pair)"));
     c->launches++;
     LBM_LAUNCHED(c, "fused step (pair)");
     return LBM_OK;

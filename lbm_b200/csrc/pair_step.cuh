@@ -461,22 +461,28 @@ __device__ __forceinline__ void pair_cell(const S* __restrict__ src, S* __restri
 #define LBM_PAIR_MIN_BLOCKS 5
 #endif
 // FP16-offset state: lower register caps (more resident warps) without spills;
-// measured best at 512x256x256: blocks of 256 threads, 4 per SM (64 registers),
-// for D3Q27, and blocks of 128, 7 per SM, for D3Q19
+// measured best at 512x256x256: 64 registers for D3Q27 (blocks of 256 threads,
+// 4 per SM, where a row's pairs fill them; else blocks of 128, 8 per SM), and
+// blocks of 128, 7 per SM, for D3Q19
 #ifndef LBM_PAIR_MIN_BLOCKS16_27
-#define LBM_PAIR_MIN_BLOCKS16_27 4
+#define LBM_PAIR_MIN_BLOCKS16_27 8
 #endif
 #ifndef LBM_PAIR_MIN_BLOCKS16_19
 #define LBM_PAIR_MIN_BLOCKS16_19 7
 #endif
-// threads per block of k_step_pair
+// the wide block of 256 threads: FP16 D3Q27 only
 template <int Q, typename S>
-__host__ __device__ constexpr int pair_threads() { return (sizeof(S) == 2 && Q == 27) ? 256 : 128; }
-// Grid: x covers nx/2 pairs in blocks of pair_threads(), y = j, z = k.  Needs
+__host__ __device__ constexpr bool pair_wide_ok() { return sizeof(S) == 2 && Q == 27; }
+// minimum resident blocks per SM for T threads per block (the register cap)
+template <int Q, typename S, int T>
+__host__ __device__ constexpr int pair_min_blocks() {
+    return sizeof(S) == 2 ? (Q == 27 ? LBM_PAIR_MIN_BLOCKS16_27 * 128 / T : LBM_PAIR_MIN_BLOCKS16_19) : LBM_PAIR_MIN_BLOCKS;
+}
+// Grid: x covers nx/2 pairs in blocks of T threads, y = j, z = k.  Needs
 // ihrr = 1 and nx even; offsets are 64-bit, so any state size.
-template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP>
-__global__ void __launch_bounds__(pair_threads<Q, S>(), sizeof(S) == 2 ? (Q == 27 ? LBM_PAIR_MIN_BLOCKS16_27 : LBM_PAIR_MIN_BLOCKS16_19) : LBM_PAIR_MIN_BLOCKS) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
-                                                                        StepArgs a) {
+template <int Q, typename S, bool WRAP, bool FORCE = false, bool FOLD = WRAP, int T = 128>
+__global__ void __launch_bounds__(T, pair_min_blocks<Q, S, T>()) k_step_pair(const S* __restrict__ src, S* __restrict__ dst,
+                                                                             StepArgs a) {
     pdl_enter();
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + 1;
     if (i > a.g.nx) return;
