@@ -117,3 +117,20 @@ def test_member_stepped_alone_is_caught():
     ens.members[0].step(1)           # back in phase
     ens.step(1)
     ens.close()
+
+
+def test_fp16_d3q27_block_shapes_match_the_ensemble():
+    """FP16 D3Q27 runs its single-domain step in blocks of 256 threads where a
+    row's pairs fill them (nx = 512 here) and of 128 otherwise (nx = 200); the
+    ensemble kernel, with its own launch shapes, must give the same bits."""
+    from lbm_b200.ensemble import build_ensemble
+    members = [W.Workload("w512", 512, 6, 5, 27, uin=0.05, lturb=True, ampl=1e-3, nrturb=3, seed=21, noise=2e-3),
+               W.Workload("w200", 200, 7, 6, 27, uin=0.04, lturb=True, ampl=1e-3, nrturb=4, seed=22, noise=2e-3)]
+    steps = 9
+    ref = [alone(wl, steps, "f16") for wl in members]
+    ens = build_ensemble(members, "f16")
+    ens.step(steps)
+    for m, got in enumerate(exported(ens)):
+        for a, b in zip(got, ref[m]):
+            assert np.array_equal(a, b), (members[m].name, float(np.abs(a - b).max()))
+    ens.close()
