@@ -534,6 +534,7 @@ __global__ void k_periodic_adj(Acc a, int axis, int nl, int skipj) {
 // disjoint sets and S is interior, so all loads can precede the stores.
 template <typename Acc>
 __global__ void __launch_bounds__(128) k_closed_adj(Acc f1, Acc f2, int axis, FacePairs lo, FacePairs hi) {
+    pdl_enter();
     const int nx = f1.g.nx, ny = f1.g.ny, nz = f1.g.nz;
     const int side = blockIdx.z;
     const FacePairs& fp = side ? hi : lo;

@@ -182,17 +182,23 @@ int lbm_state_adjoint_step(lbm_ctx* c, float* W, float* A, const void* P, int32_
         // inflow adjoint then the closed-k adjoint, with the x faces in one kernel
         const unsigned nshell = (unsigned)((sadj_shell_fold_cells(g) + 127) / 128);
         const dim3 xf((g.ny + 31) / 32, Q, g.nz);
+        // the launches of a reverse step follow one another with programmatic dependent launch
         if (Q == 27) {
-            k_sadj_shell_fold<27><<<nshell, 128, 0, c->stream>>>(W, A, g);
-            k_sadj_xface<27><<<xf, 32, 0, c->stream>>>(W, A, g, uvelhat, c->p.rho0, c->cosd, c->sind);
+            LBM_TRY(cuda_check(c, launch_pdl(k_sadj_shell_fold<27>, dim3(nshell), dim3(128), c->stream, W, A, g),
+                               "state adjoint: shell"));
+            LBM_TRY(cuda_check(c, launch_pdl(k_sadj_xface<27>, xf, dim3(32), c->stream, W, A, g, uvelhat, c->p.rho0,
+                                             c->cosd, c->sind), "state adjoint: x faces"));
         } else {
-            k_sadj_shell_fold<19><<<nshell, 128, 0, c->stream>>>(W, A, g);
-            k_sadj_xface<19><<<xf, 32, 0, c->stream>>>(W, A, g, uvelhat, c->p.rho0, c->cosd, c->sind);
+            LBM_TRY(cuda_check(c, launch_pdl(k_sadj_shell_fold<19>, dim3(nshell), dim3(128), c->stream, W, A, g),
+                               "state adjoint: shell"));
+            LBM_TRY(cuda_check(c, launch_pdl(k_sadj_xface<19>, xf, dim3(32), c->stream, W, A, g, uvelhat, c->p.rho0,
+                                             c->cosd, c->sind), "state adjoint: x faces"));
         }
         c->launches += 2;
         if (c->face_on[2]) {
-            k_closed_adj<SoaAdjAcc><<<dim3((g.nx + 127) / 128, g.ny, 2), 128, 0, c->stream>>>(a1, a2, 2, c->face[2][0],
-                                                                                           c->face[2][1]);
+            LBM_TRY(cuda_check(c, launch_pdl(k_closed_adj<SoaAdjAcc>, dim3((g.nx + 127) / 128, g.ny, 2), dim3(128),
+                                             c->stream, a1, a2, 2, c->face[2][0], c->face[2][1]),
+                               "state adjoint: closed k"));
             c->launches++;
         }
         LBM_LAUNCHED(c, "state adjoint: boundaries");
@@ -206,13 +212,16 @@ int lbm_state_adjoint_step(lbm_ctx* c, float* W, float* A, const void* P, int32_
                         : run_bc_adj<19>(c, a1, a2, uvelhat, awrap != 0));
     }
     const float* Pf = static_cast<const float*>(P);
-    if (Q == 27) {
-        if (pull) k_sadj_cell<27, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<27, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
-    } else {
-        if (pull) k_sadj_cell<19, true><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
-        else k_sadj_cell<19, false><<<inner, 128, 0, c->stream>>>(W, A, Pf, g, wrap, awrap, c->d_solid, c->cp, c->d_abl);
-    }
+    const uint8_t* sol = c->d_solid;
+    const float* abl = c->d_abl;
+    cudaError_t r;
+    if (Q == 27)
+        r = pull ? launch_pdl(k_sadj_cell<27, true>, inner, dim3(128), c->stream, W, A, Pf, g, wrap, awrap, sol, c->cp, abl)
+                 : launch_pdl(k_sadj_cell<27, false>, inner, dim3(128), c->stream, W, A, Pf, g, wrap, awrap, sol, c->cp, abl);
+    else
+        r = pull ? launch_pdl(k_sadj_cell<19, true>, inner, dim3(128), c->stream, W, A, Pf, g, wrap, awrap, sol, c->cp, abl)
+                 : launch_pdl(k_sadj_cell<19, false>, inner, dim3(128), c->stream, W, A, Pf, g, wrap, awrap, sol, c->cp, abl);
+    LBM_TRY(cuda_check(c, r, "state adjoint: collision"));
     c->launches++;
     LBM_LAUNCHED(c, "state adjoint: collision");
     return LBM_OK;

@@ -141,6 +141,7 @@ inline long long sadj_shell_cells(const SoaGrid& g, bool wrap) {
 // faces (i = 0, 1, nx, nx+1 of the rows k = 1..nz) are k_sadj_xface's.
 template <int Q>
 __global__ void __launch_bounds__(128) k_sadj_shell_fold(float* __restrict__ W, const float* __restrict__ A, SoaGrid g) {
+    pdl_enter();
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const long long nghost = 2LL * ny * (nx + 2);
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -191,6 +192,7 @@ inline long long sadj_shell_fold_cells(const SoaGrid& g) {
 template <int Q>
 __global__ void __launch_bounds__(32) k_sadj_xface(float* __restrict__ W, const float* __restrict__ A, SoaGrid g,
                                                    float* __restrict__ uvelh, float rho0, float cosd, float sind) {
+    pdl_enter();
     const int j = blockIdx.x * 32 + threadIdx.x + 1;
     const int l = blockIdx.y, k = blockIdx.z + 1;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -311,6 +313,7 @@ __global__ void __launch_bounds__(128) k_sadj_cell(float* __restrict__ W, const 
                                                    const float* __restrict__ P, SoaGrid g, int wrap, int awrap,
                                                    const uint8_t* __restrict__ solid, CollideParams cp,
                                                    const float* __restrict__ abl) {
+    pdl_enter();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y + 1, k = blockIdx.z + 1;
     if (i > g.nx) return;

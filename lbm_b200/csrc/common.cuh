@@ -75,6 +75,17 @@ __constant__ int8_t c_cz[27] = {LBM_27(LBM_CZ)};
 __constant__ int8_t c_opp[27] = {LBM_27(LBM_OPP)};
 __constant__ float c_w[2][27] = {{LBM_27(LBM_W19)}, {LBM_27(LBM_W27)}};   // [0] D3Q19, [1] D3Q27
 
+// Programmatic dependent launch (PDL) between consecutive kernels of a stream
+// (the steady step kernel and the boundary kernel, the kernels of a reverse
+// step): each kernel lets the next one in the stream be scheduled as soon as
+// all its own blocks have started, and every thread of the next one
+// waits at its start until the previous grid has completed and its memory is
+// visible.  Launched without the PDL attribute, both instructions do nothing.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Reference layout f(nl,0:nx+1,0:ny+1,0:nz+1), l fastest (Fortran column-major).
 // ---------------------------------------------------------------------------

@@ -387,15 +387,6 @@ __host__ __device__ inline long long bc_fold_xg_blocks(const SoaGrid& g, int Q, 
     return ((wide ? 2LL : (long long)Q) * g.ny * g.nz + 127) / 128;
 }
 
-// Programmatic dependent launch (PDL) between the steady step kernel and the
-// boundary kernel: each kernel lets the next one in the stream be scheduled as
-// soon as all its own blocks have started, and every thread of the next one
-// waits at its start until the previous grid has completed and its memory is
-// visible.  Launched without the PDL attribute, both instructions do nothing.
-__device__ __forceinline__ void pdl_enter() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
 
 template <int Q, typename S>
 __global__ void __launch_bounds__(128) k_bc_fold(S* f1, const S* f2, StepArgs a, int nface_blocks) {
